@@ -1,0 +1,335 @@
+"""Benchmark of the MHIT36 timestep on B200: Mpts*steps/s at 512^3 NS+ACDI.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--n 512] [--precision fp64] [--ns-only]
+
+One JSON line on rank 0.  `value` is N^3 * steps / s with the state resident
+in HBM (device-timed with CUDA events on the solver's stream, max over ranks,
+summed over replicas).  `e2e` is the same metric through the public API with
+host buffers: the upload of the state from pinned host memory, K steps each
+returning its diagnostics to the host, and the download of the state.
+
+Multi-GPU: the step does not shard (one simulation per GPU), so N ranks run N
+independent replicas of the workload ("replicas only", weak scaling); there is
+no collective on the data path.
+
+--impl reference times the CPU oracle (the C++ restatement of the
+reference's step, on all host threads) on a bounded 256^3 sample of the same
+workload recipe; the reference's own Fortran/OpenACC/cuDecomp build needs
+nvfortran and cuDecomp, which this image does not have.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "Mpts*steps/s at 512^3 NS+ACDI (FP64 plain form)"
+UNIT = "Mpts*steps/s"
+# Compulsory HBM traffic per grid point per step, FP64 NS+ACDI: 35 field passes
+# (each stage reads its inputs once and writes its outputs once).
+ALGO_BYTES_STEP = {"fp64": {True: 280, False: 232}}
+
+
+def kernel_bytes_per_point(n: int, pf: bool) -> dict:
+    """Algorithmic HBM bytes per grid point for each kernel (FP64)."""
+    spec = 16.0 * (n // 2 + 1) / n  # half spectrum, complex128
+    return {
+        "phase": 40.0,                     # read u,v,w,phi; write phi
+        "momentum": 104.0 if pf else 96.0,  # read u,v,w,rhs_o(3)[,phi]; write ustar(3), rhs_o(3)
+        "xfwd": 24.0 + spec,               # read ustar(3); write half spectrum
+        "yfwd": 2 * spec,
+        "zsolve": 2 * spec,
+        "yinv": 2 * spec,
+        "xinv": spec + 8.0,                # read spectrum; write p
+        "project": 56.0,                   # read p, ustar(3); write u,v,w
+        "finalize": 0.0,
+    }
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=512)
+    ap.add_argument("--precision", default="fp64")
+    ap.add_argument("--ns-only", action="store_true")
+    ap.add_argument("--dt", type=float, default=1e-3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload(n, pf, dt):
+    from mhit36_b200 import fields
+    from mhit36_b200.config import InputParams
+    p = InputParams(dt=dt, mu=6e-3, rho=1.0, sigma=0.5, epsr=1.0, lin_force=0.1)
+    if n >= 512:
+        recipe = (64, 0.2, 0.35)
+    else:
+        recipe = fields.DROP_RECIPES.get(n, (8, 0.4, 0.6))
+    u, v, w = fields.random_velocity(n, n)
+    phi = None
+    if pf:
+        c, r = fields.place_drops(n, n + 1, *recipe)
+        phi = fields.drop_field(n, c, r)
+    return p, (u, v, w, phi), recipe
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                rows.append(f)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def cpu_oracle_rate(n, pf, dt, case, threads=0, max_seconds=20.0, min_steps=1, max_steps=5):
+    """Time the oracle on host cores; returns (Mpts*steps/s, steps, threads)."""
+    from oracle import Oracle
+    from oracle.oracle import build_oracle
+    build_oracle()
+    p = case[0]
+    o = Oracle(n, dt=p.dt, mu=p.mu, rho=p.rho, sigma=p.sigma, epsr=p.epsr, lin_force=p.lin_force,
+               phase_field=int(pf), threads=threads)
+    u, v, w, phi = case[1]
+    o.set_fields(u, v, w, phi)
+    nthreads = o.lib.oracle_set_threads(0)
+    steps = 0
+    t0 = time.perf_counter()
+    while steps < max_steps:
+        o.step(1)
+        steps += 1
+        if steps >= min_steps and time.perf_counter() - t0 > max_seconds:
+            break
+    el = time.perf_counter() - t0
+    o.close()
+    return n ** 3 * steps / el / 1e6, steps, nthreads, el
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the CPU oracle on all host threads, rank 0 only."""
+    if rank != 0:
+        return
+    pf = not args.ns_only
+    n = min(args.n, 256)
+    case = workload(n, pf, args.dt)
+    if args.n >= 512:  # the 512^3 recipe's drops on the 256^3 sample
+        from mhit36_b200 import fields
+        if pf:
+            c, r = fields.place_drops(n, args.n + 1, 64, 0.2, 0.35)
+            case = (case[0], case[1][:3] + (fields.drop_field(n, c, r),), case[2])
+    from oracle import Oracle
+    from oracle.oracle import build_oracle
+    build_oracle()
+    p = case[0]
+    o = Oracle(n, dt=p.dt, mu=p.mu, rho=p.rho, sigma=p.sigma, epsr=p.epsr, lin_force=p.lin_force,
+               phase_field=int(pf))
+    o.set_fields(*case[1])
+    threads = o.lib.oracle_set_threads(0)
+    for _ in range(args.warmup):
+        o.step(1)
+    t0 = time.perf_counter()
+    rc, _ = o.step(args.steps)
+    el = time.perf_counter() - t0
+    value = n ** 3 * args.steps / el / 1e6
+    sample = f"{n}^3 NS{'+ACDI' if pf else ''} FP64 oracle step (512^3 recipe), {args.steps} steps"
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded random-phase velocity, seeded drops)",
+            "config": {"workload": sample, "n": n, "phase_field": pf},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "reference Fortran (nvfortran+OpenACC+cuDecomp) cannot be built in this image; "
+                    "timed: the C++ oracle restating multi/main.f90:329-977", "status": rc}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    import torch
+    import torch.distributed as dist
+    from mhit36_b200 import Solver
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    pf = not args.ns_only
+    n = args.n
+    p, case, recipe = workload(n, pf, args.dt)
+    s = Solver(n, p, precision=args.precision, phase_field=pf)
+    s.set_fields(*case)
+    stream = torch.cuda.ExternalStream(s.stream())
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # warm-up (graph capture happens here)
+    s.step(max(args.warmup, 3) if args.warmup >= 3 else args.warmup)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    s.step_async(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    diag = s.diag()
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * n ** 3 * args.steps / (ms / 1e3) / 1e6
+    launches = s.launches_per_step() * args.steps
+
+    # per-kernel durations (individually launched, CUDA events on the stream)
+    prof = s.profile_step(3)
+    kb = kernel_bytes_per_point(n, pf)
+    dominant = max(prof, key=lambda k: prof[k])
+    peak, peak_kind = peaks()
+    npts = n ** 3
+    dom_bytes = kb[dominant] * npts
+    achieved = dom_bytes / (prof[dominant] / 1e3) / 1e9
+    step_ms = ms / args.steps
+    step_bytes = ALGO_BYTES_STEP["fp64"][pf] * npts
+    roofline = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                "algo_bytes_per_launch": dom_bytes,
+                "per_kernel_ms": {k: round(v, 4) for k, v in prof.items()},
+                "per_kernel_gbs": {k: round(kb[k] * npts / (v / 1e3) / 1e9, 1) for k, v in prof.items() if kb[k]},
+                "step": {"algo_bytes_per_point": ALGO_BYTES_STEP["fp64"][pf],
+                         "achieved": step_bytes / (step_ms / 1e3) / 1e9,
+                         "frac": step_bytes / (step_ms / 1e3) / 1e9 / peak}}
+
+    # end to end through the public API with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        hb = [torch.empty(npts, dtype=torch.float64, pin_memory=True) for _ in range(4 if pf else 3)]
+        for b, src in zip(hb, case):
+            b.numpy()[:] = np.ascontiguousarray(src.T).reshape(-1)
+        ptr = [b.data_ptr() for b in hb] + ([None] if not pf else [])
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s.set_fields_ptr(*ptr)
+        for _ in range(args.steps):
+            s.step(1)  # returns the step's diagnostics to the host
+        s.get_fields_ptr(*ptr)
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        if world > 1:
+            t = torch.tensor([el], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            el = float(t.item())
+        nf = len(hb)
+        e2e = {"value": world * npts * args.steps / el / 1e6, "unit": UNIT,
+               "h2d_bytes_per_step": nf * npts * 8 / args.steps,
+               "d2h_bytes_per_step": nf * npts * 8 / args.steps + 88,
+               "ms_per_step": el / args.steps * 1e3}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, st, thr, el = cpu_oracle_rate(n, pf, args.dt, (p, case), max_seconds=20.0)
+        cpu = {"value": rate, "unit": UNIT, "cores": thr, "kind": "port",
+               "sample": f"{n}^3 NS{'+ACDI' if pf else ''} FP64, {st} oracle step(s), {el:.1f} s"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32",
+            "data": "synthetic (seeded random-phase velocity E(k)~k^4exp(-2(k/4)^2), seeded drops)",
+            "config": {"workload": f"{n}^3 NS{'+ACDI' if pf else ''} plain {args.precision} form, "
+                                   f"{recipe[0] if pf else 0} drops r in [{recipe[1]},{recipe[2]}]",
+                       "n": n, "phase_field": pf, "precision": args.precision, "dt": args.dt, "mu": 6e-3,
+                       "lin_force": 0.1, "parallelism": f"replicas x{world}",
+                       "l2": "state larger than L2 (resident fields ~{:.0f} GB)".format(s.memory_bytes() / 1e9)},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "clocks": clk, "status": diag["status"], "umax": diag["umax"], "cfl": diag["cfl"],
+        }
+        print(json.dumps(line), flush=True)
+    s.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

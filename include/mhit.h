@@ -1,0 +1,209 @@
+/*
+ * mhit.h -- C ABI of libmhit.so, a B200 (sm_100a) implementation of one
+ * MHIT36 timestep (aroccon/MHIT36).
+ *
+ * The reference has no plugin or operator API: its timestep is the body of
+ * `do t=tstart,tfin ... enddo` in program main (multi/main.f90:329-977),
+ * acting on module arrays (multi/module.f90:39-58).  These entry points
+ * replace that loop body and the field set-up/I-O around it, so a Fortran
+ * driver that keeps readinput, the field files and the time loop can call
+ * them through iso_c_binding (see fortran/mhit_iface.f90).
+ *
+ * Conventions
+ *   - Every call returns an int status (MHIT_OK = 0) and never exits.
+ *   - A handle owns its device state and one CUDA stream; it is not
+ *     thread-safe.  Distinct handles may be used concurrently.
+ *   - Host arrays are Fortran order (x fastest), float64, either the
+ *     reference's halo'd module shape (nx, ny+2, nz+2) or the raw interior
+ *     (nx, ny, nz) of the .dat files.  The caller keeps ownership.
+ */
+#ifndef MHIT_H
+#define MHIT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define MHIT_OK 0
+#define MHIT_ERR_INVALID 1     /* bad argument (size, layout, null pointer) */
+#define MHIT_ERR_CUDA 2        /* a CUDA runtime call failed */
+#define MHIT_ERR_NOMEM 3       /* device allocation failed */
+#define MHIT_ERR_CFL 4         /* CFL above the limit after a step (multi/main.f90:945 `stop`) */
+#define MHIT_ERR_NONFINITE 5   /* NaN/Inf in the velocity reductions */
+#define MHIT_ERR_IO 6          /* field file missing or of the wrong size */
+#define MHIT_ERR_UNSUPPORTED 7 /* grid size or option not built */
+#define MHIT_ERR_STATE 8       /* call out of order (e.g. step before set_fields) */
+
+/* Field layouts for set/get. */
+#define MHIT_LAYOUT_RAW 0      /* (nx, ny, nz), the .dat interior (multi/readwrite.f90:29) */
+#define MHIT_LAYOUT_PIX_HALO 1 /* (nx, ny+2, nz+2), the module arrays (multi/main.f90:184) */
+
+/* Precision forms. */
+#define MHIT_FP64 0            /* plain FP64 form */
+#define MHIT_FP32_REFINE 1     /* FP32 state + FP64-residual Poisson refinement */
+
+/* k^2 in the Poisson solve. */
+#define MHIT_K2_SPECTRAL 0     /* -(kx^2+ky^2+kz^2), integer k: the reference (multi/main.f90:791) */
+#define MHIT_K2_FD 1           /* (2/dx)^2 sum sin^2(pi m/N): exact inverse of the 7-point Laplacian */
+
+/* Grid spacing. */
+#define MHIT_GRID_REFERENCE 0  /* dx = 2pi/(nx-1) (multi/readinput.f90:37) */
+#define MHIT_GRID_CONSISTENT 1 /* dx = 2pi/nx */
+
+/*
+ * input.inp lines 1-16 (multi/readinput.f90:13-31, multi/input.inp:1-16) in
+ * order, then the switches of this implementation.  `lin_force` is an
+ * optional 17th input.inp line (linear forcing rhs += A*u); it defaults to 0,
+ * which is the reference.
+ */
+typedef struct mhit_params {
+  int32_t restart, tstart, tfin, dump; /* lines 1-4 */
+  int32_t inflow, inphi;               /* lines 5-6 */
+  double dt, mu, rho;                  /* lines 7-9 */
+  double f1, f2, f3, k0;               /* lines 10-13, ABC forcing */
+  double radius, sigma, epsr;          /* lines 14-16 */
+  double lin_force;                    /* line 17 (extension) */
+  int32_t k2_mode;                     /* MHIT_K2_* */
+  int32_t grid_mode;                   /* MHIT_GRID_* */
+  double cfl_limit;                    /* 7.0 in the reference (multi/main.f90:945) */
+  int32_t tanh_identity;               /* 1: tanh(psi/2eps) = (2phi-1)/(1+2enum); 0 = reference tanh */
+  int32_t reserved[7];
+} mhit_params;
+
+/* Per-step scalars (the values the reference prints or reduces). */
+typedef struct mhit_diag {
+  double umax;     /* gumax: signed max of u,v,w after the step (multi/main.f90:937-941) */
+  double cfl;      /* gumax*dt*dxi (multi/main.f90:942) */
+  double umean, vmean, wmean; /* means removed by the step (multi/main.f90:906-919) */
+  double gamma;    /* ACDI gamma used by the next step (1.0*gumax, multi/main.f90:362) */
+  int64_t step;    /* steps taken since set_fields/load */
+  int32_t status;  /* MHIT_OK or the sticky device error */
+  int32_t reserved;
+} mhit_diag;
+
+typedef struct mhit_handle mhit_handle;
+
+/* Fill `p` with the reference's defaults (multi/input.inp:1-16) and this
+ * implementation's defaults for the extensions. */
+void mhit_default_params(mhit_params* p);
+
+/*
+ * Create a simulation of nx*ny*nz cells on the current CUDA device.
+ * Replaces the allocation and set-up of multi/main.f90:41-200 (MPI/cuDecomp
+ * init, cuFFT plans, grid and wavenumbers, module array allocation).
+ * The reference has ny = nz = nx (multi/module.f90:2-3); so does this build.
+ * precision: MHIT_FP64 or MHIT_FP32_REFINE.  phase_field: 1 = ACDI on
+ * (`#define phiflag 1`, multi/main.f90:39), 0 = NS only.
+ */
+int mhit_create(const mhit_params* p, int nx, int ny, int nz, int precision, int phase_field,
+                mhit_handle** out);
+
+/*
+ * Upload the state from host arrays (copies; the caller keeps ownership)
+ * and reset the time-stepping state (Euler first step, gumax = 1,
+ * multi/main.f90:322-327).  phi may be NULL when phase_field = 0.
+ * Replaces readfield (multi/readwrite.f90:107-207) + the halo updates of
+ * multi/main.f90:249-260, 289-292.
+ */
+int mhit_set_fields(mhit_handle* h, const double* u, const double* v, const double* w,
+                    const double* phi, int layout);
+
+/* Download the state (any pointer may be NULL to skip that field).
+ * Halo cells of MHIT_LAYOUT_PIX_HALO are filled periodically. */
+int mhit_get_fields(mhit_handle* h, double* u, double* v, double* w, double* phi, int layout);
+
+/* Download the last pressure p (multi/main.f90:842-850). */
+int mhit_get_pressure(mhit_handle* h, double* p, int layout);
+
+/*
+ * Advance `nsteps` timesteps: the loop body of multi/main.f90:334-946 (ACDI,
+ * momentum RHS + AB2, FFT Poisson, projection, mean removal, Umax/CFL).
+ * The state stays on the device; nothing is copied back except `out`
+ * (may be NULL).  If a step ends with CFL > cfl_limit or a non-finite
+ * reduction, the remaining steps are skipped on the device and the call
+ * returns MHIT_ERR_CFL / MHIT_ERR_NONFINITE (the reference `stop`s).
+ */
+int mhit_step(mhit_handle* h, int nsteps, mhit_diag* out);
+
+/* Read the current per-step scalars without stepping. */
+int mhit_get_diag(mhit_handle* h, mhit_diag* out);
+
+/*
+ * Write output/{u,v,w,phi}_%08d.dat under `dir` in the reference's raw
+ * format (multi/readwrite.f90:1-96, called at multi/main.f90:960-971), plus
+ * a sidecar `state_%08d.bin` holding rhs_o, gumax, the pending AB2 switch and
+ * the step count, so that mhit_load resumes bit-exactly (the reference's
+ * restart re-starts with Euler and gumax = 1, multi/main.f90:241-246, 323-325).
+ */
+int mhit_save(mhit_handle* h, const char* dir, int t);
+
+/*
+ * Read fields written by mhit_save (or by the reference's writefield) at
+ * iteration t (readfield_restart, multi/readwrite.f90:218-317).  When the
+ * sidecar is present the AB2 history is restored; otherwise the next step is
+ * Euler with gumax = 1, as in the reference.
+ */
+int mhit_load(mhit_handle* h, const char* dir, int t);
+
+/*
+ * Stand-alone Poisson solve with the step's own kernels: rhs -> p on host
+ * arrays (MHIT_LAYOUT_RAW).  Replaces multi/main.f90:732-850 (rhsp ->
+ * rhsp_complex -> FFT3D -> divide by -k^2/(nx*ny*nz) -> inverse -> real part),
+ * used for the manufactured-solution check of multi/main.f90:739-741, 824-838.
+ */
+int mhit_poisson(mhit_handle* h, const double* rhs, double* p);
+
+/* Same, on device pointers (raw layout, float64), in the handle's stream. */
+int mhit_poisson_device(mhit_handle* h, const double* rhs_dev, double* p_dev);
+
+/* Device pointers of the resident state (raw layout, float64 in the FP64
+ * form; float32 in MHIT_FP32_REFINE).  For zero-copy callers; valid until the
+ * next mhit_step / mhit_destroy.  u, v, w hold the field BEFORE the pending
+ * mean removal; call mhit_sync_state first to materialise it. */
+int mhit_device_state(mhit_handle* h, void** u, void** v, void** w, void** phi);
+
+/* Apply the pending mean removal to the resident u, v, w in place. */
+int mhit_sync_state(mhit_handle* h);
+
+/* Bytes of device memory the handle holds. */
+int mhit_memory_bytes(mhit_handle* h, size_t* bytes);
+
+/* Number of kernel launches one step makes (for accounting). */
+int mhit_launches_per_step(mhit_handle* h, int* n);
+
+/*
+ * Advance `reps` steps with each kernel launched individually between CUDA
+ * events on the handle's stream and return the mean duration of every stage
+ * in ms[0..*nstages-1] (names from mhit_stage_name).  Same results as
+ * mhit_step; used for per-kernel roofline accounting.  The reference times a
+ * step with cpu_time (multi/main.f90:332, 948-949) and NVTX ranges
+ * (multi/module.f90:61-131).
+ */
+int mhit_profile_step(mhit_handle* h, int reps, double* ms, int* nstages);
+const char* mhit_stage_name(int k);
+
+/* Enqueue nsteps steps without waiting and without reading anything back. */
+int mhit_step_async(mhit_handle* h, int nsteps);
+
+/* The handle's CUDA stream (cudaStream_t) and the last CUDA error text. */
+void* mhit_stream(mhit_handle* h);
+const char* mhit_last_error(mhit_handle* h);
+
+/* Free everything (multi/main.f90:979-985). */
+int mhit_destroy(mhit_handle* h);
+
+/* Text of a status code. */
+const char* mhit_strerror(int status);
+
+/* 1 if the grid size has built kernels. */
+int mhit_size_supported(int n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MHIT_H */

@@ -1,0 +1,64 @@
+// Shared device-side definitions for libmhit (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace mhit {
+
+// Device-resident control block.  Every kernel of a step reads it instead of
+// taking step-dependent scalars as launch arguments, so one captured CUDA graph
+// replays every step.
+struct Ctrl {
+  double mean[3];       // mean still to be removed from the stored u, v, w
+  double gumax;         // signed Umax of the last step; gamma = 1.0*gumax
+  double alpha, beta;   // AB2 weights of the next step (1, 0 before step 1)
+  double cfl;           // gumax*dt*dxi of the last step
+  double cfl_limit;     // step error above this (7 in the reference)
+  double last_mean[3];  // means removed by the last step
+  long long nstep;      // steps taken
+  int status;           // sticky MHIT_* error; kernels return early when set
+  int pad_;
+};
+
+// Scalars fixed for the life of a handle, passed by value.
+struct StepConst {
+  int n;
+  int abc;            // ABC forcing active
+  int tanh_identity;  // tanh(psi/2eps) from phi directly
+  int pad_;
+  double dt, mu, rho, rhoi, dxi, ddxi, eps, epsi, enumv, tiny, sigma, lin_force;
+  double f1, f2, f3;
+  double cdiv;        // rho*dxi/dt   (multi/main.f90:723)
+  double dtr;         // dt/rho       (multi/main.f90:881)
+};
+
+__device__ __forceinline__ int wrapi(int a, int n) { return a < 0 ? a + n : (a >= n ? a - n : a); }
+
+__device__ __forceinline__ size_t gidx(int i, int j, int k, int n) {
+  return (size_t)i + (size_t)n * ((size_t)j + (size_t)n * (size_t)k);
+}
+
+// ---- complex helpers (double2 / float2) ----
+template <class T> struct C2;
+template <> struct C2<double> { typedef double2 t; };
+template <> struct C2<float> { typedef float2 t; };
+
+template <class C> __device__ __forceinline__ C cadd(C a, C b) { C r; r.x = a.x + b.x; r.y = a.y + b.y; return r; }
+template <class C> __device__ __forceinline__ C csub(C a, C b) { C r; r.x = a.x - b.x; r.y = a.y - b.y; return r; }
+template <class C> __device__ __forceinline__ C cmul(C a, C b) {
+  C r; r.x = a.x * b.x - a.y * b.y; r.y = a.x * b.y + a.y * b.x; return r;
+}
+// a * conj(b)
+template <class C> __device__ __forceinline__ C cmulc(C a, C b) {
+  C r; r.x = a.x * b.x + a.y * b.y; r.y = a.y * b.x - a.x * b.y; return r;
+}
+template <class C> __device__ __forceinline__ C cconj(C a) { C r; r.x = a.x; r.y = -a.y; return r; }
+template <class C, class T> __device__ __forceinline__ C cscale(C a, T s) { C r; r.x = a.x * s; r.y = a.y * s; return r; }
+// multiply by (DIR * i)
+template <int DIR, class C> __device__ __forceinline__ C cmul_i(C a) {
+  C r;
+  if (DIR > 0) { r.x = -a.y; r.y = a.x; } else { r.x = a.y; r.y = -a.x; }
+  return r;
+}
+
+}  // namespace mhit

@@ -1,0 +1,152 @@
+// Shared-memory batched FFT for libmhit.
+//
+// A CTA holds L complex lines of length N in shared memory, interleaved so
+// that element n of line l sits at s[n*L + l] ("column-major": the L lines
+// are the fast axis).  That is the layout of a chunk of L consecutive kx
+// columns of the spectrum, so the y and z passes stage 128-byte rows straight
+// from HBM, and every Stockham stage below reads and writes 32 consecutive
+// elements per warp (no shared-memory bank conflicts for 8- or 16-byte
+// elements).
+//
+// The transform is the Stockham autosort formulation (natural-order output,
+// in place through registers): for each stage with radix R and span Ns,
+//   v[r] = x[j + r*N/R] * w_N^(DIR * r*(j mod Ns)*N/(Ns*R)),  v = DFT_R(v),
+//   x'[(j/Ns)*Ns*R + (j mod Ns) + r*Ns] = v[r].
+// DIR = -1 is the forward transform e^{-2 pi i jk/N} (cuFFT's
+// CUFFT_FORWARD, used by the reference at multi/main.f90:750-761), DIR = +1
+// the unnormalised inverse (multi/main.f90:802-812).  Twiddles come from a
+// table tw[m] = e^{-2 pi i m/N} computed on the host in long double.
+#pragma once
+#include "common.cuh"
+
+namespace mhit {
+
+constexpr int pick_radix(int rem) {
+  return rem % 8 == 0 ? 8 : (rem % 4 == 0 ? 4 : (rem % 2 == 0 ? 2 : (rem % 3 == 0 ? 3 : rem)));
+}
+
+template <int R, int DIR, class C> struct DFT;
+
+template <int DIR, class C> struct DFT<2, DIR, C> {
+  static __device__ __forceinline__ void run(C* v) {
+    C a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  }
+};
+
+template <int DIR, class C> __device__ __forceinline__ void dft4(C& a0, C& a1, C& a2, C& a3) {
+  C t0 = cadd(a0, a2), t1 = csub(a0, a2), t2 = cadd(a1, a3), t3 = cmul_i<DIR>(csub(a1, a3));
+  a0 = cadd(t0, t2);
+  a2 = csub(t0, t2);
+  a1 = cadd(t1, t3);
+  a3 = csub(t1, t3);
+}
+
+template <int DIR, class C> struct DFT<4, DIR, C> {
+  static __device__ __forceinline__ void run(C* v) { dft4<DIR>(v[0], v[1], v[2], v[3]); }
+};
+
+template <int DIR, class C> struct DFT<8, DIR, C> {
+  static __device__ __forceinline__ void run(C* v) {
+    typedef decltype(v[0].x) T;
+    const T h = (T)0.70710678118654752440084436210484903928;
+    C e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+    C o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+    dft4<DIR>(e0, e1, e2, e3);
+    dft4<DIR>(o0, o1, o2, o3);
+    // w8^1 = h(1 + DIR i), w8^2 = DIR i, w8^3 = h(-1 + DIR i)
+    C t1, t3;
+    t1.x = h * (o1.x - (T)DIR * o1.y);
+    t1.y = h * (o1.y + (T)DIR * o1.x);
+    C t2 = cmul_i<DIR>(o2);
+    t3.x = h * (-o3.x - (T)DIR * o3.y);
+    t3.y = h * (-o3.y + (T)DIR * o3.x);
+    v[0] = cadd(e0, o0);
+    v[4] = csub(e0, o0);
+    v[1] = cadd(e1, t1);
+    v[5] = csub(e1, t1);
+    v[2] = cadd(e2, t2);
+    v[6] = csub(e2, t2);
+    v[3] = cadd(e3, t3);
+    v[7] = csub(e3, t3);
+  }
+};
+
+template <int DIR, class C> struct DFT<3, DIR, C> {
+  static __device__ __forceinline__ void run(C* v) {
+    typedef decltype(v[0].x) T;
+    const T s3 = (T)0.86602540378443864676372317075293618347;  // sqrt(3)/2
+    C a = v[0], b = v[1], c = v[2];
+    C t1 = cadd(b, c);
+    C t2;
+    t2.x = a.x - (T)0.5 * t1.x;
+    t2.y = a.y - (T)0.5 * t1.y;
+    C d = cmul_i<DIR>(cscale(csub(b, c), s3));
+    v[0] = cadd(a, t1);
+    v[1] = cadd(t2, d);
+    v[2] = csub(t2, d);
+  }
+};
+
+template <class C> __device__ __forceinline__ C ldg_c(const C* p) { return __ldg(p); }
+
+// One Stockham stage over L interleaved lines, NT threads.
+template <int N, int R, int NS, int L, int NT, int DIR, class C>
+__device__ __forceinline__ void fft_stage(C* s, const C* __restrict__ tw) {
+  constexpr int NR = N / R;
+  constexpr int W = L * NR;
+  constexpr int ITEMS = (W + NT - 1) / NT;
+  constexpr int TSTRIDE = N / (NS * R);
+  C v[ITEMS][R];
+#pragma unroll
+  for (int it = 0; it < ITEMS; ++it) {
+    const int wi = threadIdx.x + it * NT;
+    if ((ITEMS * NT == W) || wi < W) {
+      const int l = wi % L, j = wi / L;
+      const int jm = j % NS;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        C a = s[(j + r * NR) * L + l];
+        if (NS > 1 && r > 0) {
+          C t = ldg_c(tw + r * jm * TSTRIDE);
+          a = (DIR < 0) ? cmul(a, t) : cmulc(a, t);
+        }
+        v[it][r] = a;
+      }
+      DFT<R, DIR, C>::run(v[it]);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int it = 0; it < ITEMS; ++it) {
+    const int wi = threadIdx.x + it * NT;
+    if ((ITEMS * NT == W) || wi < W) {
+      const int l = wi % L, j = wi / L;
+      const int jm = j % NS;
+      const int d0 = (j / NS) * NS * R + jm;
+#pragma unroll
+      for (int r = 0; r < R; ++r) s[(d0 + r * NS) * L + l] = v[it][r];
+    }
+  }
+  __syncthreads();
+}
+
+template <int N, int NS, int L, int NT, int DIR, class C> struct FFTRun {
+  static __device__ __forceinline__ void run(C* s, const C* __restrict__ tw) {
+    if constexpr (NS < N) {
+      constexpr int R = pick_radix(N / NS);
+      fft_stage<N, R, NS, L, NT, DIR, C>(s, tw);
+      FFTRun<N, NS * R, L, NT, DIR, C>::run(s, tw);
+    }
+  }
+};
+
+// In-place transform of L interleaved lines of length N held in s.
+// Must be called by all NT threads of the CTA; ends with a barrier.
+template <int N, int L, int NT, int DIR, class C>
+__device__ __forceinline__ void smem_fft(C* s, const C* __restrict__ tw) {
+  FFTRun<N, 1, L, NT, DIR, C>::run(s, tw);
+}
+
+}  // namespace mhit

@@ -1,0 +1,499 @@
+// Stencil kernels of the MHIT36 step on one B200: the ACDI phase-field update,
+// the momentum RHS + AB2 predictor, the projection with the mean/max
+// reductions, and the one-block finalize.
+//
+// Fields are stored without halo cells, x fastest (n^3 values); periodic
+// neighbours come from index wrap.  On one rank this is exactly what the
+// reference's cuDecomp halo updates (periodic, multi/main.f90:418-429,
+// 483-486, 630-641, 685-696, 817-818, 923-934) provide, so none of the 28 halo
+// calls of a reference step has a counterpart here.
+//
+// Both stencil kernels march a TX x TY column tile through a chunk of KZ z
+// planes ("2.5D" blocking): each z plane of every input is read from HBM once
+// per tile (plus its x/y halo ring, mostly L2 hits), kept in a small ring of
+// shared-memory planes, and every intermediate the reference materialises in
+// HBM (psidi, normx/y/z, rhsphi, rhsu/v/w, chempot, gradphi*, f*st) lives
+// only in shared memory or registers.
+#include <cuda_runtime.h>
+#include <math.h>
+#include "common.cuh"
+#include "internal.h"
+
+namespace mhit {
+
+constexpr int TX = 32, TY = 8, NT = TX * TY;
+
+static int pick_kz(int n) { return n >= 32 ? 32 : n; }
+
+// ============================================================ phase field
+// ACDI step A1..A7 (multi/main.f90:341-480) fused into one kernel:
+//   psi = eps*log((min(phi,1)+enum)/(1-min(phi,1)+enum))      (A3)
+//   n   = grad(psi) / (|grad(psi)| + 1e-16f)                  (A4, A5)
+//   F   = 0.25*(1 - tanh(psi/(2 eps))^2) * n                  (A6 flux)
+//   rhs = -div(u phi_face) + gamma*eps*lap(phi) - gamma*div_c(F)   (A1, A2, A6)
+//   phi_new = phi + dt*rhs                                    (A7)
+// psi needs phi on a radius-2 neighbourhood; it is computed per plane on the
+// tile plus a 2-cell ring, F on the tile plus a 1-cell ring.
+template <class T>
+__global__ void __launch_bounds__(NT) phase_kernel(StencilArgs<T> a, int KZ) {
+  if (a.ctrl->status) return;
+  constexpr int EX = TX + 4, EY = TY + 4, PE = EX * EY;
+  constexpr int FX = TX + 2, FY = TY + 2, FE = FX * FY;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* s_phi = reinterpret_cast<T*>(smem_raw);  // ring of 5 planes
+  T* s_psi = s_phi + 5 * PE;                  // ring of 3 planes
+  T* s_F = s_psi + 3 * PE;                    // ring of 3 planes x 3 components
+  const int n = a.c.n;
+  const T eps = (T)a.c.eps, epsi = (T)a.c.epsi, enumv = (T)a.c.enumv, tiny = (T)a.c.tiny;
+  const T dxi = (T)a.c.dxi, ddxi = (T)a.c.ddxi, dt = (T)a.c.dt;
+  const T gamma = (T)(1.0 * a.ctrl->gumax);  // multi/main.f90:362
+  const T mu = (T)a.ctrl->mean[0], mv = (T)a.ctrl->mean[1], mw = (T)a.ctrl->mean[2];
+  const int use_ident = a.c.tanh_identity;
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, k0 = blockIdx.z * KZ;
+  const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
+  const int i = x0 + tx, j = y0 + ty;
+  const int ip = (i + 1 == n) ? 0 : i + 1, jp = (j + 1 == n) ? 0 : j + 1;
+  const size_t nn = (size_t)n * n;
+
+  for (int m = k0 - 2; m <= k0 + KZ + 1; ++m) {
+    // (1) phi plane m on the tile + 2 ring, and psi there.
+    {
+      T* Pphi = s_phi + ((m + 15) % 5) * PE;
+      T* Ppsi = s_psi + ((m + 15) % 3) * PE;
+      const T* src = a.phi_in + (size_t)wrapi(m, n) * nn;
+      for (int e = tid; e < PE; e += NT) {
+        const int ex = e % EX, ey = e / EX;
+        const int gx = wrapi(x0 - 2 + ex, n), gy = wrapi(y0 - 2 + ey, n);
+        const T f = src[gx + (size_t)n * gy];
+        Pphi[e] = f;
+        const T val = fmin(f, (T)1);
+        Ppsi[e] = eps * log((val + enumv) / ((T)1 - val + enumv));
+      }
+    }
+    __syncthreads();
+    // (2) F on plane m-1 over the tile + 1 ring.
+    if (m >= k0) {
+      const int fm = m - 1;
+      const T* Pc = s_psi + ((fm + 15) % 3) * PE;
+      const T* Pm = s_psi + ((fm + 14) % 3) * PE;
+      const T* Pp = s_psi + ((fm + 16) % 3) * PE;
+      const T* Phc = s_phi + ((fm + 15) % 5) * PE;
+      T* F = s_F + ((fm + 15) % 3) * 3 * FE;
+      for (int e = tid; e < FE; e += NT) {
+        const int fx = e % FX, fy = e / FX;
+        const int pe = (fx + 1) + (fy + 1) * EX;
+        const T gxv = Pc[pe + 1] - Pc[pe - 1];
+        const T gyv = Pc[pe + EX] - Pc[pe - EX];
+        const T gzv = Pp[pe] - Pm[pe];
+        const T normod = (T)1 / (sqrt(gxv * gxv + gyv * gyv + gzv * gzv) + tiny);
+        T t;
+        if (use_ident) {
+          const T val = fmin(Phc[pe], (T)1);
+          t = ((T)2 * val - (T)1) / ((T)1 + (T)2 * enumv);
+        } else {
+          t = tanh((T)0.5 * Pc[pe] * epsi);
+        }
+        const T g = (T)0.25 * ((T)1 - t * t);
+        F[e] = g * (gxv * normod);
+        F[FE + e] = g * (gyv * normod);
+        F[2 * FE + e] = g * (gzv * normod);
+      }
+    }
+    __syncthreads();
+    // (3) output plane k = m-2.
+    if (m >= k0 + 2) {
+      const int k = m - 2;
+      const int kz = wrapi(k, n), kzp = wrapi(k + 1, n);
+      const T* P0 = s_phi + ((k + 15) % 5) * PE;
+      const T* Pm1 = s_phi + ((k + 14) % 5) * PE;
+      const T* Pp1 = s_phi + ((k + 16) % 5) * PE;
+      const T* F0 = s_F + ((k + 15) % 3) * 3 * FE;
+      const T* Fm = s_F + ((k + 14) % 3) * 3 * FE;
+      const T* Fp = s_F + ((k + 16) % 3) * 3 * FE;
+      const int pe = (tx + 2) + (ty + 2) * EX;
+      const int fe = (tx + 1) + (ty + 1) * FX;
+      const T c = P0[pe], pxp = P0[pe + 1], pxm = P0[pe - 1], pyp = P0[pe + EX], pym = P0[pe - EX];
+      const T pzp = Pp1[pe], pzm = Pm1[pe];
+      const size_t g = (size_t)i + (size_t)n * j + nn * kz;
+      const T uc = a.u[g] - mu, uxp = a.u[(size_t)ip + (size_t)n * j + nn * kz] - mu;
+      const T vc = a.v[g] - mv, vyp = a.v[(size_t)i + (size_t)n * jp + nn * kz] - mv;
+      const T wc = a.w[g] - mw, wzp = a.w[(size_t)i + (size_t)n * j + nn * kzp] - mw;
+      const T h = (T)0.5;
+      T r = -(uxp * h * (pxp + c) - uc * h * (c + pxm)) * dxi - (vyp * h * (pyp + c) - vc * h * (c + pym)) * dxi -
+            (wzp * h * (pzp + c) - wc * h * (c + pzm)) * dxi;
+      r = r + gamma * (eps * (pxp - (T)2 * c + pxm) * ddxi + eps * (pyp - (T)2 * c + pym) * ddxi +
+                       eps * (pzp - (T)2 * c + pzm) * ddxi);
+      r = r - gamma * ((F0[fe + 1] - F0[fe - 1]) * h * dxi + (F0[FE + fe + FX] - F0[FE + fe - FX]) * h * dxi +
+                       (Fp[2 * FE + fe] - Fm[2 * FE + fe]) * h * dxi);
+      a.phi_out[g] = c + dt * r;
+    }
+  }
+}
+
+// ============================================================ momentum
+// B1..B7 (multi/main.f90:513-682) fused: conservative convection, viscous
+// term, ABC forcing, optional linear forcing A*u, surface tension
+// f = 6 sigma chempot grad(phi) at cell centres interpolated to the faces,
+// and the AB2 (Euler on the first step) predictor.  Writes ustar and the new
+// rhs_o; reads the NEW phi (the reference computes B4 after A7).
+template <class T, bool PF>
+__global__ void __launch_bounds__(NT) momentum_kernel(StencilArgs<T> a, int KZ) {
+  if (a.ctrl->status) return;
+  constexpr int UX = TX + 2, UY = TY + 2, UE = UX * UY;  // velocity planes, 1-cell ring
+  constexpr int EX = TX + 4, EY = TY + 4, PE = EX * EY;  // phi planes, 2-cell ring
+  constexpr int QX = TX + 1, QY = TY + 1, QE = QX * QY;  // force over [-1,TX) x [-1,TY)
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* s_u = reinterpret_cast<T*>(smem_raw);  // ring of 4 planes each
+  T* s_v = s_u + 4 * UE;
+  T* s_w = s_v + 4 * UE;
+  T* s_phi = s_w + 4 * UE;     // ring of 4 (PF only)
+  T* s_f = s_phi + 4 * PE;     // ring of 2 planes x 3 components (PF only)
+  const int n = a.c.n;
+  const T dxi = (T)a.c.dxi, ddxi = (T)a.c.ddxi, dt = (T)a.c.dt, mu_v = (T)a.c.mu, rhoi = (T)a.c.rhoi;
+  const T eps = (T)a.c.eps, epsi = (T)a.c.epsi, sig6 = (T)(6.0 * a.c.sigma), lin = (T)a.c.lin_force;
+  const T f1 = (T)a.c.f1, f2 = (T)a.c.f2, f3 = (T)a.c.f3;
+  const T alpha = (T)a.ctrl->alpha, beta = (T)a.ctrl->beta;
+  const T mu = (T)a.ctrl->mean[0], mv = (T)a.ctrl->mean[1], mw = (T)a.ctrl->mean[2];
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, k0 = blockIdx.z * KZ;
+  const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
+  const int i = x0 + tx, j = y0 + ty;
+  const size_t nn = (size_t)n * n;
+  const T h = (T)0.5, q = (T)0.25;
+
+  for (int m = k0 - 2; m <= k0 + KZ; ++m) {
+    const int mz = wrapi(m, n);
+    {
+      const int sl = (m + 8) & 3;
+      T* Su = s_u + sl * UE;
+      T* Sv = s_v + sl * UE;
+      T* Sw = s_w + sl * UE;
+      const size_t zoff = (size_t)mz * nn;
+      for (int e = tid; e < UE; e += NT) {
+        const int ex = e % UX, ey = e / UX;
+        const size_t gg = zoff + (size_t)wrapi(x0 - 1 + ex, n) + (size_t)n * wrapi(y0 - 1 + ey, n);
+        Su[e] = a.u[gg] - mu;
+        Sv[e] = a.v[gg] - mv;
+        Sw[e] = a.w[gg] - mw;
+      }
+      if (PF) {
+        T* Sp = s_phi + sl * PE;
+        for (int e = tid; e < PE; e += NT) {
+          const int ex = e % EX, ey = e / EX;
+          Sp[e] = a.phi_in[zoff + (size_t)wrapi(x0 - 2 + ex, n) + (size_t)n * wrapi(y0 - 2 + ey, n)];
+        }
+      }
+    }
+    __syncthreads();
+    if (PF && m >= k0) {
+      // B4: chempot, grad(phi), f at plane m-1 (multi/main.f90:617-623)
+      const int fm = m - 1;
+      const T* P0 = s_phi + ((fm + 8) & 3) * PE;
+      const T* Pm = s_phi + ((fm + 7) & 3) * PE;
+      const T* Pp = s_phi + ((fm + 9) & 3) * PE;
+      T* F = s_f + ((fm + 8) & 1) * 3 * QE;
+      for (int e = tid; e < QE; e += NT) {
+        const int qx = e % QX, qy = e / QX;
+        const int pe = (qx + 1) + (qy + 1) * EX;
+        const T c = P0[pe], pxp = P0[pe + 1], pxm = P0[pe - 1], pyp = P0[pe + EX], pym = P0[pe - EX];
+        const T pzp = Pp[pe], pzm = Pm[pe];
+        const T chem = c * ((T)1 - c) * ((T)1 - (T)2 * c) * epsi -
+                       eps * (pxp + pxm + pyp + pym + pzp + pzm - (T)6 * c) * ddxi;
+        const T gx = h * (pxp - pxm) * dxi, gy = h * (pyp - pym) * dxi, gz = h * (pzp - pzm) * dxi;
+        F[e] = sig6 * chem * gx;
+        F[QE + e] = sig6 * chem * gy;
+        F[2 * QE + e] = sig6 * chem * gz;
+      }
+    }
+    if (PF) __syncthreads();
+    if (m >= k0 + 1) {
+      const int k = m - 1;
+      const T* U0 = s_u + ((k + 8) & 3) * UE;
+      const T* Um = s_u + ((k + 7) & 3) * UE;
+      const T* Up = s_u + ((k + 9) & 3) * UE;
+      const T* V0 = s_v + ((k + 8) & 3) * UE;
+      const T* Vm = s_v + ((k + 7) & 3) * UE;
+      const T* Vp = s_v + ((k + 9) & 3) * UE;
+      const T* W0 = s_w + ((k + 8) & 3) * UE;
+      const T* Wm = s_w + ((k + 7) & 3) * UE;
+      const T* Wp = s_w + ((k + 9) & 3) * UE;
+      const int e = (tx + 1) + (ty + 1) * UX;
+      const T uc = U0[e], uxp = U0[e + 1], uxm = U0[e - 1], uyp = U0[e + UX], uym = U0[e - UX];
+      const T uzp = Up[e], uzm = Um[e], uxpym = U0[e + 1 - UX], uxpzm = Um[e + 1];
+      const T vc = V0[e], vxp = V0[e + 1], vxm = V0[e - 1], vyp = V0[e + UX], vym = V0[e - UX];
+      const T vzp = Vp[e], vzm = Vm[e], vxmyp = V0[e - 1 + UX], vypzm = Vm[e + UX];
+      const T wc = W0[e], wxp = W0[e + 1], wxm = W0[e - 1], wyp = W0[e + UX], wym = W0[e - UX];
+      const T wzp = Wp[e], wzm = Wm[e], wxmzp = Wp[e - 1], wymzp = Wp[e - UX];
+      // B1 (multi/main.f90:527-549)
+      T h11 = (uxp + uc) * (uxp + uc) - (uc + uxm) * (uc + uxm);
+      T h12 = (uyp + uc) * (vyp + vxmyp) - (uc + uym) * (vc + vxm);
+      T h13 = (uzp + uc) * (wzp + wxmzp) - (uc + uzm) * (wc + wxm);
+      T h21 = (uxp + uxpym) * (vxp + vc) - (uc + uym) * (vc + vxm);
+      T h22 = (vyp + vc) * (vyp + vc) - (vc + vym) * (vc + vym);
+      T h23 = (wzp + wymzp) * (vzp + vc) - (wc + wym) * (vc + vzm);
+      T h31 = (wxp + wc) * (uxp + uxpzm) - (wc + wxm) * (uc + uzm);
+      T h32 = (vyp + vypzm) * (wyp + wc) - (vc + vzm) * (wc + wym);
+      T h33 = (wzp + wc) * (wzp + wc) - (wc + wzm) * (wc + wzm);
+      h11 = h11 * q * dxi; h12 = h12 * q * dxi; h13 = h13 * q * dxi;
+      h21 = h21 * q * dxi; h22 = h22 * q * dxi; h23 = h23 * q * dxi;
+      h31 = h31 * q * dxi; h32 = h32 * q * dxi; h33 = h33 * q * dxi;
+      T ru = -(h11 + h12 + h13);
+      T rv = -(h21 + h22 + h23);
+      T rw = -(h31 + h32 + h33);
+      // B2 (multi/main.f90:567-578)
+      h11 = mu_v * (uxp - (T)2 * uc + uxm) * ddxi;
+      h12 = mu_v * (uyp - (T)2 * uc + uym) * ddxi;
+      h13 = mu_v * (uzp - (T)2 * uc + uzm) * ddxi;
+      h21 = mu_v * (vxp - (T)2 * vc + vxm) * ddxi;
+      h22 = mu_v * (vyp - (T)2 * vc + vym) * ddxi;
+      h23 = mu_v * (vzp - (T)2 * vc + vzm) * ddxi;
+      h31 = mu_v * (wxp - (T)2 * wc + wxm) * ddxi;
+      h32 = mu_v * (wyp - (T)2 * wc + wym) * ddxi;
+      h33 = mu_v * (wzp - (T)2 * wc + wzm) * ddxi;
+      ru = ru + (h11 + h12 + h13) * rhoi;
+      rv = rv + (h21 + h22 + h23) * rhoi;
+      rw = rw + (h31 + h32 + h33) * rhoi;
+      const int kz = wrapi(k, n);
+      // B3 ABC forcing (multi/main.f90:591-593), global interior coordinates
+      if (a.c.abc) {
+        ru = ru + f3 * (T)a.fsin[kz] + f2 * (T)a.fcos[j];
+        rv = rv + f1 * (T)a.fsin[i] + f3 * (T)a.fcos[kz];
+        rw = rw + f2 * (T)a.fsin[j] + f1 * (T)a.fcos[i];
+      }
+      if (lin != (T)0) {  // linear forcing (extension)
+        ru = ru + lin * uc;
+        rv = rv + lin * vc;
+        rw = rw + lin * wc;
+      }
+      if (PF) {  // B5 (multi/main.f90:652-654)
+        const T* F0 = s_f + ((k + 8) & 1) * 3 * QE;
+        const T* Fm = s_f + ((k + 7) & 1) * 3 * QE;
+        const int qe = (tx + 1) + (ty + 1) * QX;
+        ru = ru + h * (F0[qe - 1] + F0[qe]) * rhoi;
+        rv = rv + h * (F0[QE + qe - QX] + F0[QE + qe]) * rhoi;
+        rw = rw + h * (Fm[2 * QE + qe] + F0[2 * QE + qe]) * rhoi;
+      }
+      // B6, B7 (multi/main.f90:666-681)
+      const size_t g = (size_t)i + (size_t)n * j + nn * kz;
+      const T ruo = a.ru[g], rvo = a.rv[g], rwo = a.rw[g];
+      a.us[g] = uc + dt * (alpha * ru - beta * ruo);
+      a.vs[g] = vc + dt * (alpha * rv - beta * rvo);
+      a.ws[g] = wc + dt * (alpha * rw - beta * rwo);
+      a.ru[g] = ru;
+      a.rv[g] = rv;
+      a.rw[g] = rw;
+    }
+  }
+}
+
+// ============================================================ projection
+// C2 + R1 (multi/main.f90:873-903): u = ustar - dt/rho*(p - p_m)*dxi, with the
+// sums and maxima of the projected u, v, w reduced per CTA in FP64.
+constexpr int PKZ = 16;
+
+template <class T>
+__global__ void __launch_bounds__(NT) project_kernel(StencilArgs<T> a) {
+  if (a.ctrl->status) return;
+  const int n = a.c.n;
+  const T dtr = (T)a.c.dtr, dxi = (T)a.c.dxi;
+  const int i = blockIdx.x * TX + threadIdx.x % TX, j = blockIdx.y * TY + threadIdx.x / TX;
+  const int k0 = blockIdx.z * PKZ;
+  const int im = i ? i - 1 : n - 1, jm = j ? j - 1 : n - 1;
+  const size_t nn = (size_t)n * n;
+  double su = 0, sv = 0, sw = 0;
+  double xu = -INFINITY, xv = -INFINITY, xw = -INFINITY;
+  T pprev = a.p[(size_t)i + (size_t)n * j + nn * wrapi(k0 - 1, n)];
+  for (int k = k0; k < k0 + PKZ; ++k) {
+    const size_t g = (size_t)i + (size_t)n * j + nn * k;
+    const T pc = a.p[g];
+    const T uo = a.us[g] - dtr * (pc - a.p[g - i + im]) * dxi;
+    const T vo = a.vs[g] - dtr * (pc - a.p[g + (size_t)n * jm - (size_t)n * j]) * dxi;
+    const T wo = a.ws[g] - dtr * (pc - pprev) * dxi;
+    pprev = pc;
+    a.uo[g] = uo;
+    a.vo[g] = vo;
+    a.wo[g] = wo;
+    su += (double)uo;
+    sv += (double)vo;
+    sw += (double)wo;
+    xu = fmax(xu, (double)uo);
+    xv = fmax(xv, (double)vo);
+    xw = fmax(xw, (double)wo);
+    // NaN must not vanish in fmax: fold it into the sums too
+    if (uo != uo || vo != vo || wo != wo) su = NAN;
+  }
+  // deterministic block reduction: xor-shuffle in warps, then warps in order
+  double vals[6] = {su, sv, sw, xu, xv, xw};
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+    for (int t = 0; t < 3; ++t) vals[t] += __shfl_xor_sync(0xffffffffu, vals[t], o);
+#pragma unroll
+    for (int t = 3; t < 6; ++t) vals[t] = fmax(vals[t], __shfl_xor_sync(0xffffffffu, vals[t], o));
+  }
+  __shared__ double red[NT / 32][6];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) {
+#pragma unroll
+    for (int t = 0; t < 6; ++t) red[wid][t] = vals[t];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double r[6];
+#pragma unroll
+    for (int t = 0; t < 6; ++t) r[t] = red[0][t];
+    for (int w = 1; w < NT / 32; ++w) {
+      for (int t = 0; t < 3; ++t) r[t] += red[w][t];
+      for (int t = 3; t < 6; ++t) r[t] = fmax(r[t], red[w][t]);
+    }
+    const size_t b = (size_t)blockIdx.x + (size_t)gridDim.x * (blockIdx.y + (size_t)gridDim.y * blockIdx.z);
+    for (int t = 0; t < 6; ++t) a.partials[b * 6 + t] = r[t];
+  }
+}
+
+// ============================================================ finalize
+// M1, C3, R2 and the CFL guard (multi/main.f90:906-946), one CTA:
+// means = sum/nx/ny/nz, removed lazily (stored in ctrl->mean and subtracted by
+// every reader of u, v, w); gumax = max(max(u)-um, max(v)-vm, max(w)-wm), which
+// equals the reference's max of the mean-removed fields because rounding is
+// monotonic; then gamma, CFL, AB2 switch and the sticky error status.
+constexpr int FNT = 1024;
+
+__global__ void __launch_bounds__(FNT) finalize_kernel(const double* __restrict__ partials, int nparts, Ctrl* ctrl,
+                                                       StepConst c) {
+  if (ctrl->status) return;
+  double v[6] = {0, 0, 0, -INFINITY, -INFINITY, -INFINITY};
+  for (int b = threadIdx.x; b < nparts; b += FNT) {
+    for (int t = 0; t < 3; ++t) v[t] += partials[(size_t)b * 6 + t];
+    for (int t = 3; t < 6; ++t) v[t] = fmax(v[t], partials[(size_t)b * 6 + t]);
+  }
+  __shared__ double red[FNT][6];
+  for (int t = 0; t < 6; ++t) red[threadIdx.x][t] = v[t];
+  __syncthreads();
+  for (int s = FNT / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      for (int t = 0; t < 3; ++t) red[threadIdx.x][t] += red[threadIdx.x + s][t];
+      for (int t = 3; t < 6; ++t) red[threadIdx.x][t] = fmax(red[threadIdx.x][t], red[threadIdx.x + s][t]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double nd = (double)c.n;
+    const double um = red[0][0] / nd / nd / nd;
+    const double vm = red[0][1] / nd / nd / nd;
+    const double wm = red[0][2] / nd / nd / nd;
+    const double uc = red[0][3] - um, vc = red[0][4] - vm, wc = red[0][5] - wm;
+    const double umax = fmax(wc, fmax(uc, vc));
+    const double cou = umax * c.dt * c.dxi;
+    ctrl->mean[0] = um;
+    ctrl->mean[1] = vm;
+    ctrl->mean[2] = wm;
+    ctrl->last_mean[0] = um;
+    ctrl->last_mean[1] = vm;
+    ctrl->last_mean[2] = wm;
+    ctrl->gumax = umax;
+    ctrl->cfl = cou;
+    ctrl->alpha = 1.5;
+    ctrl->beta = 0.5;
+    ctrl->nstep += 1;
+    const double s = red[0][0] + red[0][1] + red[0][2];
+    if (!isfinite(s) || !isfinite(umax)) ctrl->status = 5;  // MHIT_ERR_NONFINITE
+    else if (cou > ctrl->cfl_limit) ctrl->status = 4;      // MHIT_ERR_CFL
+  }
+}
+
+// u -= mean in place, then mean = 0 (materialises the lazy mean removal).
+template <class T>
+__global__ void materialize_kernel(T* u, T* v, T* w, size_t count, Ctrl* ctrl) {
+  const T mu = (T)ctrl->mean[0], mv = (T)ctrl->mean[1], mw = (T)ctrl->mean[2];
+  for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < count; g += (size_t)gridDim.x * blockDim.x) {
+    u[g] = u[g] - mu;
+    v[g] = v[g] - mv;
+    w[g] = w[g] - mw;
+  }
+}
+
+__global__ void clear_mean_kernel(Ctrl* ctrl) {
+  ctrl->mean[0] = 0;
+  ctrl->mean[1] = 0;
+  ctrl->mean[2] = 0;
+}
+
+// ============================================================ launchers
+template <class T> static size_t phase_smem() {
+  return sizeof(T) * (size_t)(8 * (TX + 4) * (TY + 4) + 9 * (TX + 2) * (TY + 2));
+}
+template <class T> static size_t momentum_smem(bool pf) {
+  size_t s = 3 * 4 * (TX + 2) * (TY + 2);
+  if (pf) s += 4 * (TX + 4) * (TY + 4) + 2 * 3 * (TX + 1) * (TY + 1);
+  return sizeof(T) * s;
+}
+
+int stencil_size_ok(int n) { return n >= 32 && n % TX == 0 && n % TY == 0 && n % PKZ == 0 && n % pick_kz(n) == 0; }
+
+int project_partials(int n) { return (n / TX) * (n / TY) * (n / PKZ); }
+
+template <class T> static cudaError_t prep_t() {
+  cudaError_t e;
+  if ((e = cudaFuncSetAttribute(phase_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)phase_smem<T>())))
+    return e;
+  if ((e = cudaFuncSetAttribute(momentum_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)momentum_smem<T>(true))))
+    return e;
+  if ((e = cudaFuncSetAttribute(momentum_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)momentum_smem<T>(false))))
+    return e;
+  return cudaSuccess;
+}
+
+cudaError_t prepare_stencils() {
+  cudaError_t e = prep_t<double>();
+  if (e) return e;
+  return prep_t<float>();
+}
+
+template <class T> cudaError_t launch_phase(const StencilArgs<T>& a, cudaStream_t st) {
+  const int n = a.c.n, kz = pick_kz(n);
+  dim3 grid(n / TX, n / TY, n / kz);
+  phase_kernel<T><<<grid, NT, phase_smem<T>(), st>>>(a, kz);
+  return cudaGetLastError();
+}
+
+template <class T> cudaError_t launch_momentum(const StencilArgs<T>& a, bool pf, cudaStream_t st) {
+  const int n = a.c.n, kz = pick_kz(n);
+  dim3 grid(n / TX, n / TY, n / kz);
+  if (pf)
+    momentum_kernel<T, true><<<grid, NT, momentum_smem<T>(true), st>>>(a, kz);
+  else
+    momentum_kernel<T, false><<<grid, NT, momentum_smem<T>(false), st>>>(a, kz);
+  return cudaGetLastError();
+}
+
+template <class T> cudaError_t launch_project(const StencilArgs<T>& a, cudaStream_t st) {
+  const int n = a.c.n;
+  dim3 grid(n / TX, n / TY, n / PKZ);
+  project_kernel<T><<<grid, NT, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_finalize(const double* partials, int nparts, Ctrl* ctrl, StepConst c, cudaStream_t st) {
+  finalize_kernel<<<1, FNT, 0, st>>>(partials, nparts, ctrl, c);
+  return cudaGetLastError();
+}
+
+template <class T> cudaError_t launch_materialize(T* u, T* v, T* w, int n, Ctrl* ctrl, cudaStream_t st) {
+  const size_t count = (size_t)n * n * n;
+  materialize_kernel<T><<<1184, 256, 0, st>>>(u, v, w, count, ctrl);
+  clear_mean_kernel<<<1, 1, 0, st>>>(ctrl);
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_phase<double>(const StencilArgs<double>&, cudaStream_t);
+template cudaError_t launch_phase<float>(const StencilArgs<float>&, cudaStream_t);
+template cudaError_t launch_momentum<double>(const StencilArgs<double>&, bool, cudaStream_t);
+template cudaError_t launch_momentum<float>(const StencilArgs<float>&, bool, cudaStream_t);
+template cudaError_t launch_project<double>(const StencilArgs<double>&, cudaStream_t);
+template cudaError_t launch_project<float>(const StencilArgs<float>&, cudaStream_t);
+template cudaError_t launch_materialize<double>(double*, double*, double*, int, Ctrl*, cudaStream_t);
+template cudaError_t launch_materialize<float>(float*, float*, float*, int, Ctrl*, cudaStream_t);
+
+}  // namespace mhit

@@ -1,0 +1,168 @@
+"""CPU tests of the host side: input.inp, field files, seeded inputs, and the
+C ABI library's exports (no compute call needs a GPU here)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+INPUT_INP_REF_STYLE = """0           ! fresh start=0 restart =1
+0           ! iteration to start from (fresh start 0 otherwise different)
+20000       ! Final time step
+1000        ! Saving frequency
+0           ! inflow condition (0=Taylor green, 1=read from fields)
+0           ! phase-field initial condition (0=circular drop, 1=read from fields)
+0.0002      ! dt for the simulation
+0.006       ! mu (viscosity)
+1.000       ! density
+0.0         ! A forcing parameter (ABC forcing)
+0.0         ! B forcing parameter (ABC forcing)
+0.0         ! C forcing parameter (ABC forcing)
+2.0         ! Forced wavenumber (ABC forcing)
+0.5         ! Initial drop radius for phase-field
+1.0d0       ! Surface tension
+1.0         ! Ratio eps/dx
+"""
+
+
+def test_read_input_reference_format(tmp_path):
+    from mhit36_b200.config import read_input
+    p = tmp_path / "input.inp"
+    p.write_text(INPUT_INP_REF_STYLE)
+    prm = read_input(str(p))
+    assert (prm.restart, prm.tstart, prm.tfin, prm.dump, prm.inflow, prm.inphi) == (0, 0, 20000, 1000, 0, 0)
+    assert (prm.dt, prm.mu, prm.rho) == (0.0002, 0.006, 1.0)
+    assert (prm.f1, prm.f2, prm.f3, prm.k0) == (0.0, 0.0, 0.0, 2.0)
+    assert (prm.radius, prm.sigma, prm.epsr) == (0.5, 1.0, 1.0)  # "1.0d0" is a Fortran double literal
+    assert prm.lin_force == 0.0
+    # optional 17th line: linear forcing
+    p.write_text(INPUT_INP_REF_STYLE + "0.1   ! linear forcing A\n")
+    assert read_input(str(p)).lin_force == 0.1
+
+
+def test_input_roundtrip_and_derived(tmp_path):
+    from mhit36_b200.config import InputParams, read_input, write_input
+    prm = InputParams(tfin=200, dt=1e-3, mu=6e-3, sigma=0.5, lin_force=0.1, inflow=1, inphi=1)
+    write_input(str(tmp_path / "input.inp"), prm)
+    back = read_input(str(tmp_path / "input.inp"))
+    for k in ("tfin", "dt", "mu", "sigma", "lin_force", "inflow", "inphi", "rho", "epsr"):
+        assert getattr(back, k) == getattr(prm, k)
+    d = prm.derived(128)
+    assert d["dx"] == 8.0 * np.arctan(1.0) / 127  # multi/readinput.f90:37
+    assert d["enum"] == float(np.float32(1e-16))
+
+
+def test_field_file_roundtrip(tmp_path):
+    from mhit36_b200 import fields
+    n = 8
+    a = np.random.default_rng(0).standard_normal((n, n, n))
+    path = str(tmp_path / "u.dat")
+    fields.write_field(path, a)
+    raw = np.fromfile(path, dtype="<f8")
+    assert raw.size == n ** 3
+    assert raw[1] == a[1, 0, 0] and raw[n] == a[0, 1, 0] and raw[n * n] == a[0, 0, 1]  # x fastest
+    assert np.array_equal(fields.read_field(path, n), a)
+    with pytest.raises(ValueError):
+        fields.read_field(path, n + 1)
+    assert fields.output_name("out", 5, 12) == os.path.join("out", "phi_00000012.dat")
+
+
+def test_random_velocity_properties():
+    from mhit36_b200 import fields
+    n = 32
+    u, v, w = fields.random_velocity(n, seed=n)
+    for f in (u, v, w):
+        assert abs(f.mean()) < 1e-14
+    rms = np.sqrt((np.mean(u ** 2) + np.mean(v ** 2) + np.mean(w ** 2)) / 3)
+    assert abs(rms - 1.0) < 1e-12
+    # solenoidal in index space once the half-cell stagger is undone
+    k = np.fft.fftfreq(n, 1.0 / n)
+    U = np.fft.fftn(u) * np.exp(1j * np.pi * k / n)[:, None, None]
+    V = np.fft.fftn(v) * np.exp(1j * np.pi * k / n)[None, :, None]
+    W = np.fft.fftn(w) * np.exp(1j * np.pi * k / n)[None, None, :]
+    div = k[:, None, None] * U + k[None, :, None] * V + k[None, None, :] * W
+    assert np.max(np.abs(div)) / np.max(np.abs(U)) < 1e-10
+    # seeded: same seed, same field
+    u2, _, _ = fields.random_velocity(n, seed=n)
+    assert np.array_equal(u, u2)
+
+
+def test_drop_field_recipe():
+    from mhit36_b200 import fields
+    n = 64
+    c, r = fields.place_drops(n, seed=n + 1, ndrops=4, rmin=0.4, rmax=0.6)
+    dx = fields.grid_dx(n)
+    period = n * dx
+    for a in range(4):
+        for b in range(a):
+            d = c[a] - c[b]
+            d -= period * np.round(d / period)
+            assert np.linalg.norm(d) > r[a] + r[b] + 4 * dx
+    phi = fields.drop_field(n, c, r)
+    assert phi.min() >= 0 and phi.max() <= 1
+    vol = phi.sum() * dx ** 3
+    # 0.5(1 - tanh((d-r)/2eps)) = 1/(1+exp((d-r)/eps)): volume (4pi/3)(r^3 + pi^2 eps^2 r)
+    eps = dx
+    ref = 4 / 3 * np.pi * (r ** 3 + np.pi ** 2 * eps ** 2 * r).sum()
+    assert abs(vol / ref - 1) < 0.02
+
+
+def test_centred_drop_matches_reference_formula():
+    from mhit36_b200 import fields
+    n = 16
+    phi = fields.centred_drop(n, 0.5)
+    dx = 2 * np.pi / (n - 1)
+    x = np.arange(n) * dx
+    i, j, k = 3, 7, 11
+    pos = (x[i] - np.pi) ** 2 + (x[j] - np.pi) ** 2 + (x[k] - np.pi) ** 2
+    assert phi[i, j, k] == 0.5 * (1 - np.tanh((np.sqrt(pos) - 0.5) / 2 / dx))
+
+
+def _header_functions():
+    txt = open(os.path.join(ROOT, "include", "mhit.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(mhit_[a-z_0-9]+)\s*\(", txt)))
+
+
+def test_library_exports_every_header_symbol():
+    from mhit36_b200 import capi
+    lib = capi.load_library()
+    names = _header_functions()
+    assert set(capi.HEADER_SYMBOLS) <= set(names)
+    for name in names:
+        assert hasattr(lib, name), name
+    # pure host calls, no GPU needed
+    assert lib.mhit_strerror(capi.MHIT_ERR_CFL).decode() == "CFL above the limit"
+    assert lib.mhit_size_supported(512) == 1
+    assert lib.mhit_size_supported(500) == 0
+    p = capi.MhitParams()
+    lib.mhit_default_params(ctypes.byref(p))
+    assert (p.dt, p.mu, p.tfin, p.cfl_limit) == (0.0002, 0.006, 20000, 7.0)  # multi/input.inp
+
+
+def test_params_struct_layout_matches_header():
+    """The ctypes mirror and the C struct agree on size (checked with gcc)."""
+    import subprocess
+    import tempfile
+    from mhit36_b200 import capi
+    src = '#include "mhit.h"\n#include <stdio.h>\nint main(){printf("%zu %zu\\n", sizeof(mhit_params), sizeof(mhit_diag));return 0;}\n'
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "s.c")
+        open(c, "w").write(src)
+        exe = os.path.join(d, "s")
+        subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), c, "-o", exe], check=True)
+        a, b = map(int, subprocess.run([exe], capture_output=True, text=True).stdout.split())
+    assert a == ctypes.sizeof(capi.MhitParams)
+    assert b == ctypes.sizeof(capi.MhitDiag)
+
+
+def test_create_without_gpu_fails_cleanly():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("GPU present")
+    from mhit36_b200 import Solver, MhitError
+    with pytest.raises(MhitError):
+        Solver(32, phase_field=False)
