@@ -68,7 +68,11 @@ def parse():
     ap.add_argument("--n", type=int, default=512)
     ap.add_argument("--precision", default="fp64")
     ap.add_argument("--ns-only", action="store_true")
-    ap.add_argument("--dt", type=float, default=1e-3)
+    # The explicit ACDI diffusion gamma*eps*lap(phi) (gamma = Umax, eps = dx) is
+    # stable only for Umax*dt/dx < 1/6; at 512^3 with Umax ~ 4 that needs
+    # dt < 5e-4.  The default is the reference's own input.inp dt (2e-4);
+    # throughput does not depend on dt.
+    ap.add_argument("--dt", type=float, default=2e-4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
@@ -235,7 +239,7 @@ def main():
             dist.barrier()
 
     # warm-up (graph capture happens here)
-    s.step(max(args.warmup, 3) if args.warmup >= 3 else args.warmup)
+    s.step(args.warmup)
     torch.cuda.synchronize()
     clocks = ClockSampler(local)
     barrier()

@@ -80,10 +80,22 @@ typedef struct mhit_diag {
   double cfl;      /* gumax*dt*dxi (multi/main.f90:942) */
   double umean, vmean, wmean; /* means removed by the step (multi/main.f90:906-919) */
   double gamma;    /* ACDI gamma used by the next step (1.0*gumax, multi/main.f90:362) */
+  double max_div;  /* FP32 refine form: max |div u| of the FP64 projection; -1 in the FP64 form */
   int64_t step;    /* steps taken since set_fields/load */
   int32_t status;  /* MHIT_OK or the sticky device error */
   int32_t reserved;
 } mhit_diag;
+
+/* FP64 diagnostics of the resident state (mhit_diagnostics). */
+typedef struct mhit_stats {
+  double ke;          /* 0.5 <u^2 + v^2 + w^2> over the cells */
+  double dissipation; /* 2 nu <S_ij S_ij>, centred differences (post/compute_diss/main.f90:72-117) */
+  double max_div;     /* max |forward-difference div u| (the projection's operator, multi/main.f90:723-725) */
+  double phi_sum;     /* sum of phi over the cells (volume / dx^3) */
+  double phi_min, phi_max;
+  double umean;       /* mean of u after the pending mean removal */
+  double reserved;
+} mhit_stats;
 
 typedef struct mhit_handle mhit_handle;
 
@@ -128,6 +140,15 @@ int mhit_get_pressure(mhit_handle* h, double* p, int layout);
  * returns MHIT_ERR_CFL / MHIT_ERR_NONFINITE (the reference `stop`s).
  */
 int mhit_step(mhit_handle* h, int nsteps, mhit_diag* out);
+
+/*
+ * FP64 diagnostics of the current state, computed on the GPU: kinetic energy,
+ * viscous dissipation as the reference's post-processor computes it
+ * (post/compute_diss/main.f90:72-117; pi_f32 = 1 uses its float32-rounded pi,
+ * post/compute_diss/module.f90:5, with dx = 2 pi/(nx-1); pi_f32 = 0 uses the
+ * grid's own dx), max |div u|, and the phi volume sum and bounds.
+ */
+int mhit_diagnostics(mhit_handle* h, int pi_f32, mhit_stats* out);
 
 /* Read the current per-step scalars without stepping. */
 int mhit_get_diag(mhit_handle* h, mhit_diag* out);
@@ -184,7 +205,7 @@ int mhit_launches_per_step(mhit_handle* h, int* n);
  * (multi/module.f90:61-131).
  */
 int mhit_profile_step(mhit_handle* h, int reps, double* ms, int* nstages);
-const char* mhit_stage_name(int k);
+const char* mhit_stage_name(mhit_handle* h, int k);
 
 /* Enqueue nsteps steps without waiting and without reading anything back. */
 int mhit_step_async(mhit_handle* h, int nsteps);

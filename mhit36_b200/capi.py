@@ -48,9 +48,17 @@ class MhitDiag(ctypes.Structure):
     _fields_ = [
         ("umax", ctypes.c_double), ("cfl", ctypes.c_double),
         ("umean", ctypes.c_double), ("vmean", ctypes.c_double), ("wmean", ctypes.c_double),
-        ("gamma", ctypes.c_double),
+        ("gamma", ctypes.c_double), ("max_div", ctypes.c_double),
         ("step", ctypes.c_int64), ("status", ctypes.c_int32), ("reserved", ctypes.c_int32),
     ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+class MhitStats(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_double) for k in
+                ("ke", "dissipation", "max_div", "phi_sum", "phi_min", "phi_max", "umean", "reserved")]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
@@ -62,7 +70,7 @@ HEADER_SYMBOLS = [
     "mhit_step", "mhit_get_diag", "mhit_save", "mhit_load", "mhit_poisson", "mhit_poisson_device",
     "mhit_device_state", "mhit_sync_state", "mhit_memory_bytes", "mhit_launches_per_step",
     "mhit_destroy", "mhit_strerror", "mhit_size_supported", "mhit_profile_step", "mhit_stage_name",
-    "mhit_step_async", "mhit_stream", "mhit_last_error",
+    "mhit_step_async", "mhit_stream", "mhit_last_error", "mhit_diagnostics",
 ]
 
 _lib = None
@@ -104,7 +112,8 @@ def load_library(path: str = LIB_PATH):
         "mhit_last_error": (ctypes.c_char_p, [H]),
         "mhit_stream": (ctypes.c_void_p, [H]),
         "mhit_profile_step": (ctypes.c_int, [H, ctypes.c_int, P(ctypes.c_double), P(ctypes.c_int)]),
-        "mhit_stage_name": (ctypes.c_char_p, [ctypes.c_int]),
+        "mhit_stage_name": (ctypes.c_char_p, [H, ctypes.c_int]),
+        "mhit_diagnostics": (ctypes.c_int, [H, ctypes.c_int, P(MhitStats)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -11,6 +11,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -33,10 +34,23 @@ struct mhit_handle {
   double* p = nullptr;
   double2* spec = nullptr;
   double2* tw = nullptr;
+  // FP32 refinement form state (u, v, w, ustar, rhs_o, phi in FP32; the
+  // Poisson solve is an FP32 solve p0 plus an FP32 correction solve dp of the
+  // FP64 residual)
+  float *fu = nullptr, *fv = nullptr, *fw = nullptr;
+  float *fus = nullptr, *fvs = nullptr, *fws = nullptr;
+  float *fru = nullptr, *frv = nullptr, *frw = nullptr;
+  float* fphi[2] = {nullptr, nullptr};
+  float *fp0 = nullptr, *fdp = nullptr;
+  float2* fspec = nullptr;
+  float2* ftw = nullptr;
   double* k2tab = nullptr;
   double *fsin = nullptr, *fcos = nullptr;
   double* partials = nullptr;
   int nparts = 0;
+  double* stat_partials = nullptr;
+  double* stat_out = nullptr;
+  double* h_stat = nullptr;  // pinned
   Ctrl* ctrl = nullptr;
   Ctrl* h_ctrl = nullptr;  // pinned mirror
   long long nstep_host = 0;
@@ -89,6 +103,7 @@ void free_all(mhit_handle* h) {
   for (void* q : h->allocs) cudaFree(q);
   h->allocs.clear();
   if (h->h_ctrl) cudaFreeHost(h->h_ctrl);
+  if (h->h_stat) cudaFreeHost(h->h_stat);
   if (h->st) cudaStreamDestroy(h->st);
 }
 
@@ -100,43 +115,114 @@ bool size_supported(int n) {
   return built && mhit::stencil_size_ok(n);
 }
 
-mhit::StencilArgs<double> stencil_args(mhit_handle* h, int cur) {
-  mhit::StencilArgs<double> a;
-  a.u = h->u; a.v = h->v; a.w = h->w;
-  a.phi_in = h->phi[cur];
-  a.phi_out = h->phi[cur ^ 1];
-  a.us = h->us; a.vs = h->vs; a.ws = h->ws;
-  a.ru = h->ru; a.rv = h->rv; a.rw = h->rw;
-  a.p = h->p;
-  a.uo = h->u; a.vo = h->v; a.wo = h->w;
+template <class T> struct Buffers;
+template <> struct Buffers<double> {
+  static mhit::StencilArgs<double> args(mhit_handle* h, int cur) {
+    mhit::StencilArgs<double> a;
+    a.u = h->u; a.v = h->v; a.w = h->w;
+    a.phi_in = h->phi[cur];
+    a.phi_out = h->phi[cur ^ 1];
+    a.us = h->us; a.vs = h->vs; a.ws = h->ws;
+    a.ru = h->ru; a.rv = h->rv; a.rw = h->rw;
+    a.p = h->p;
+    a.uo = h->u; a.vo = h->v; a.wo = h->w;
+    return a;
+  }
+};
+template <> struct Buffers<float> {
+  static mhit::StencilArgs<float> args(mhit_handle* h, int cur) {
+    mhit::StencilArgs<float> a;
+    a.u = h->fu; a.v = h->fv; a.w = h->fw;
+    a.phi_in = h->fphi[cur];
+    a.phi_out = h->fphi[cur ^ 1];
+    a.us = h->fus; a.vs = h->fvs; a.ws = h->fws;
+    a.ru = h->fru; a.rv = h->frv; a.rw = h->frw;
+    a.p = h->fp0;
+    a.uo = h->fu; a.vo = h->fv; a.wo = h->fw;
+    return a;
+  }
+};
+
+template <class T> mhit::StencilArgs<T> stencil_args(mhit_handle* h, int cur) {
+  mhit::StencilArgs<T> a = Buffers<T>::args(h, cur);
   a.partials = h->partials;
-  a.fsin = h->fsin; a.fcos = h->fcos;
+  a.fsin = h->fsin;
+  a.fcos = h->fcos;
   a.ctrl = h->ctrl;
   a.c = h->c;
   return a;
 }
 
-// Enqueue the kernels of one step reading phi[cur] (9 launches with ACDI).
-cudaError_t enqueue_step(mhit_handle* h, int cur) {
-  mhit::StencilArgs<double> a = stencil_args(h, cur);
-  cudaError_t e;
-  if (h->phase_field) {
-    if ((e = mhit::launch_phase<double>(a, h->st))) return e;
-    a.phi_in = h->phi[cur ^ 1];  // momentum reads the updated phi
+typedef std::pair<const char*, std::function<cudaError_t()>> Stage;
+
+// The kernels of one step reading phi[cur], in launch order.
+//   FP64: [phase] momentum xfwd yfwd zsolve yinv xinv project finalize
+//   FP32 refine: [phase] momentum, solve 1 (xfwd yfwd zsolve yinv xinv -> p0),
+//     solve 2 of the FP64 residual (xres yfwd2 zsolve2 yinv2 xinv2 -> dp),
+//     project (FP64), finalize
+std::vector<Stage> step_stages(mhit_handle* h, int cur) {
+  std::vector<Stage> v;
+  cudaStream_t st = h->st;
+  const int n = h->n;
+  const bool pf = h->phase_field != 0;
+  static const char* pnames[5] = {"xfwd", "yfwd", "zsolve", "yinv", "xinv"};
+  static const char* rnames[5] = {"xres", "yfwd2", "zsolve2", "yinv2", "xinv2"};
+  if (h->precision == MHIT_FP64) {
+    mhit::StencilArgs<double> a = stencil_args<double>(h, cur);
+    mhit::StencilArgs<double> am = a;
+    if (pf) {
+      v.push_back({"phase", [a, st] { return mhit::launch_phase<double>(a, st); }});
+      am.phi_in = h->phi[cur ^ 1];  // momentum reads the updated phi
+    }
+    v.push_back({"momentum", [am, pf, st] { return mhit::launch_momentum<double>(am, pf, st); }});
+    mhit::PoissonArgs<double> pa;
+    pa.us = h->us; pa.vs = h->vs; pa.ws = h->ws;
+    pa.spec = h->spec; pa.p = h->p; pa.tw = h->tw; pa.k2tab = h->k2tab; pa.ctrl = h->ctrl;
+    pa.cdiv = h->c.cdiv; pa.ddxi = h->c.ddxi;
+    for (int k = 0; k < 5; ++k)
+      v.push_back({pnames[k], [pa, n, k, st] { return mhit::launch_poisson_stage<double>(n, pa, k, st); }});
+    v.push_back({"project", [a, st] { return mhit::launch_project<double>(a, st); }});
+    Ctrl* ctrl = h->ctrl;
+    double* part = h->partials;
+    int np = h->nparts;
+    StepConst c = h->c;
+    v.push_back({"finalize", [part, np, ctrl, c, st] { return mhit::launch_finalize(part, np, 6, ctrl, c, st); }});
+  } else {
+    mhit::StencilArgs<float> a = stencil_args<float>(h, cur);
+    mhit::StencilArgs<float> am = a;
+    if (pf) {
+      v.push_back({"phase", [a, st] { return mhit::launch_phase<float>(a, st); }});
+      am.phi_in = h->fphi[cur ^ 1];
+    }
+    v.push_back({"momentum", [am, pf, st] { return mhit::launch_momentum<float>(am, pf, st); }});
+    mhit::PoissonArgs<float> pa;
+    pa.us = h->fus; pa.vs = h->fvs; pa.ws = h->fws;
+    pa.spec = h->fspec; pa.p = h->fp0; pa.tw = h->ftw; pa.k2tab = h->k2tab; pa.ctrl = h->ctrl;
+    pa.cdiv = h->c.cdiv; pa.ddxi = h->c.ddxi;
+    for (int k = 0; k < 5; ++k)
+      v.push_back({pnames[k], [pa, n, k, st] { return mhit::launch_poisson_stage<float>(n, pa, k, st); }});
+    mhit::PoissonArgs<float> pr = pa;
+    pr.pres = h->fp0;  // residual r - L(p0) in FP64
+    pr.p = h->fdp;
+    for (int k = 0; k < 5; ++k)
+      v.push_back({rnames[k], [pr, n, k, st] { return mhit::launch_poisson_stage<float>(n, pr, k, st); }});
+    float* dp = h->fdp;
+    v.push_back({"project", [a, dp, st] { return mhit::launch_project_refine(a, dp, st); }});
+    Ctrl* ctrl = h->ctrl;
+    double* part = h->partials;
+    int np = h->nparts;
+    StepConst c = h->c;
+    v.push_back({"finalize", [part, np, ctrl, c, st] { return mhit::launch_finalize(part, np, 7, ctrl, c, st); }});
   }
-  if ((e = mhit::launch_momentum<double>(a, h->phase_field != 0, h->st))) return e;
-  mhit::PoissonArgs<double> pa;
-  pa.us = h->us; pa.vs = h->vs; pa.ws = h->ws;
-  pa.rhs = nullptr;
-  pa.spec = h->spec;
-  pa.p = h->p;
-  pa.tw = h->tw;
-  pa.k2tab = h->k2tab;
-  pa.ctrl = h->ctrl;
-  pa.cdiv = h->c.cdiv;
-  if ((e = mhit::launch_poisson<double>(h->n, pa, h->st))) return e;
-  if ((e = mhit::launch_project<double>(a, h->st))) return e;
-  return mhit::launch_finalize(h->partials, h->nparts, h->ctrl, h->c, h->st);
+  return v;
+}
+
+cudaError_t enqueue_step(mhit_handle* h, int cur) {
+  for (auto& stg : step_stages(h, cur)) {
+    cudaError_t e = stg.second();
+    if (e) return e;
+  }
+  return cudaSuccess;
 }
 
 cudaError_t build_graph(mhit_handle* h, int cur) {
@@ -191,6 +277,61 @@ cudaError_t download(mhit_handle* h, double* dst, const double* src, int layout)
   return cudaSuccess;
 }
 
+// A device field of either form: FP64 or FP32 storage, raw layout.
+struct DevField {
+  void* ptr;
+  bool f32;
+};
+
+// host float64 (layout) -> device field; FP32 fields are rounded on the host.
+cudaError_t put_field(mhit_handle* h, DevField d, const double* src, int layout) {
+  if (!d.f32) return upload(h, static_cast<double*>(d.ptr), src, layout);
+  const int n = h->n;
+  const size_t plane = (size_t)n * n;
+  std::vector<float> tmp(plane * n);
+  for (int k = 0; k < n; ++k) {
+    const double* s = (layout == MHIT_LAYOUT_RAW) ? src + plane * k : src + (size_t)n * (1 + (size_t)(n + 2) * (k + 1));
+    float* t = tmp.data() + plane * k;
+    for (size_t q = 0; q < plane; ++q) t[q] = (float)s[q];
+  }
+  cudaError_t e = cudaMemcpyAsync(d.ptr, tmp.data(), tmp.size() * sizeof(float), cudaMemcpyHostToDevice, h->st);
+  if (e) return e;
+  return cudaStreamSynchronize(h->st);  // tmp dies here
+}
+
+// device field -> host float64 (layout); synchronous for FP32 fields.
+cudaError_t get_field(mhit_handle* h, double* dst, DevField d, int layout) {
+  if (!d.f32) return download(h, dst, static_cast<const double*>(d.ptr), layout);
+  const int n = h->n;
+  const size_t plane = (size_t)n * n;
+  std::vector<float> tmp(plane * n);
+  cudaError_t e = cudaMemcpyAsync(tmp.data(), d.ptr, tmp.size() * sizeof(float), cudaMemcpyDeviceToHost, h->st);
+  if (e) return e;
+  if ((e = cudaStreamSynchronize(h->st))) return e;
+  for (int k = 0; k < n; ++k) {
+    double* t = (layout == MHIT_LAYOUT_RAW) ? dst + plane * k : dst + (size_t)n * (1 + (size_t)(n + 2) * (k + 1));
+    const float* s = tmp.data() + plane * k;
+    for (size_t q = 0; q < plane; ++q) t[q] = (double)s[q];
+  }
+  return cudaSuccess;
+}
+
+bool f32(mhit_handle* h) { return h->precision == MHIT_FP32_REFINE; }
+DevField fu(mhit_handle* h) { return f32(h) ? DevField{h->fu, true} : DevField{h->u, false}; }
+DevField fv(mhit_handle* h) { return f32(h) ? DevField{h->fv, true} : DevField{h->v, false}; }
+DevField fw(mhit_handle* h) { return f32(h) ? DevField{h->fw, true} : DevField{h->w, false}; }
+DevField fphi(mhit_handle* h, int cur) { return f32(h) ? DevField{h->fphi[cur], true} : DevField{h->phi[cur], false}; }
+DevField frhs_o(mhit_handle* h, int q) {
+  if (f32(h)) return DevField{q == 0 ? h->fru : (q == 1 ? h->frv : h->frw), true};
+  return DevField{q == 0 ? h->ru : (q == 1 ? h->rv : h->rw), false};
+}
+size_t elem_size(mhit_handle* h) { return f32(h) ? sizeof(float) : sizeof(double); }
+
+cudaError_t materialize(mhit_handle* h) {
+  if (f32(h)) return mhit::launch_materialize<float>(h->fu, h->fv, h->fw, h->n, h->ctrl, h->st);
+  return mhit::launch_materialize<double>(h->u, h->v, h->w, h->n, h->ctrl, h->st);
+}
+
 // Periodic halo fill of a host (nx, ny+2, nz+2) array (after download).
 void fill_halo_host(double* a, int n) {
   const size_t row = (size_t)n, sy = (size_t)n + 2;
@@ -212,6 +353,7 @@ void fill_diag(mhit_handle* h, mhit_diag* d) {
   d->vmean = c->last_mean[1];
   d->wmean = c->last_mean[2];
   d->gamma = 1.0 * c->gumax;
+  d->max_div = c->max_div;
   d->step = c->nstep;
   d->status = c->status;
   d->reserved = 0;
@@ -267,7 +409,10 @@ int mhit_create(const mhit_params* p, int nx, int ny, int nz, int precision, int
   *out = nullptr;
   if (nx != ny || nx != nz) return MHIT_ERR_UNSUPPORTED;  // ny = nz = nx (multi/module.f90:2-3)
   if (!size_supported(nx)) return MHIT_ERR_UNSUPPORTED;
-  if (precision != MHIT_FP64) return MHIT_ERR_UNSUPPORTED;
+  if (precision != MHIT_FP64 && precision != MHIT_FP32_REFINE) return MHIT_ERR_UNSUPPORTED;
+  // One FP32 correction solve converges only when the solve inverts the FD
+  // Laplacian exactly, i.e. with the FD-modified k^2.
+  if (precision == MHIT_FP32_REFINE && p->k2_mode != MHIT_K2_FD) return MHIT_ERR_UNSUPPORTED;
   if (!(p->dt > 0) || !(p->rho > 0) || !(p->epsr > 0)) return MHIT_ERR_INVALID;
   mhit_handle* h = new mhit_handle();
   h->n = nx;
@@ -311,23 +456,48 @@ int mhit_create(const mhit_params* p, int nx, int ny, int nz, int precision, int
     if ((e = mhit::prepare_poisson(n))) { fail(e, "prepare_poisson"); break; }
     if ((e = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking))) { fail(e, "stream"); break; }
     const size_t N3 = (size_t)n * n * n;
-    const size_t fb = N3 * sizeof(double);
-    double** fields[] = {&h->u, &h->v, &h->w, &h->us, &h->vs, &h->ws, &h->ru, &h->rv, &h->rw, &h->p};
-    bool bad = false;
-    for (double** f : fields) {
-      if ((e = dalloc(h, f, fb))) { fail(e, "cudaMalloc field"); bad = true; break; }
-    }
-    if (bad) break;
-    if (h->phase_field) {
-      if ((e = dalloc(h, &h->phi[0], fb)) || (e = dalloc(h, &h->phi[1], fb))) { fail(e, "cudaMalloc phi"); break; }
-    }
     const size_t pitch = mhit::spectrum_pitch(n);
-    const size_t sb = (size_t)n * n * pitch * sizeof(double2);
-    if ((e = dalloc(h, &h->spec, sb))) { fail(e, "cudaMalloc spectrum"); break; }
-    if ((e = cudaMemsetAsync(h->spec, 0, sb, h->st))) { fail(e, "memset"); break; }
+    bool bad = false;
+    if (precision == MHIT_FP64) {
+      const size_t fb = N3 * sizeof(double);
+      double** fields[] = {&h->u, &h->v, &h->w, &h->us, &h->vs, &h->ws, &h->ru, &h->rv, &h->rw, &h->p};
+      for (double** f : fields) {
+        if ((e = dalloc(h, f, fb))) { fail(e, "cudaMalloc field"); bad = true; break; }
+      }
+      if (bad) break;
+      if (h->phase_field) {
+        if ((e = dalloc(h, &h->phi[0], fb)) || (e = dalloc(h, &h->phi[1], fb))) { fail(e, "cudaMalloc phi"); break; }
+      }
+      const size_t sb = (size_t)n * n * pitch * sizeof(double2);
+      if ((e = dalloc(h, &h->spec, sb))) { fail(e, "cudaMalloc spectrum"); break; }
+      if ((e = cudaMemsetAsync(h->spec, 0, sb, h->st))) { fail(e, "memset"); break; }
+    } else {
+      const size_t fb = N3 * sizeof(float);
+      float** fields[] = {&h->fu, &h->fv, &h->fw, &h->fus, &h->fvs, &h->fws, &h->fru, &h->frv, &h->frw,
+                          &h->fp0, &h->fdp};
+      for (float** f : fields) {
+        if ((e = dalloc(h, f, fb))) { fail(e, "cudaMalloc field"); bad = true; break; }
+      }
+      if (bad) break;
+      if (h->phase_field) {
+        if ((e = dalloc(h, &h->fphi[0], fb)) || (e = dalloc(h, &h->fphi[1], fb))) { fail(e, "cudaMalloc phi"); break; }
+      }
+      const size_t sb = (size_t)n * n * pitch * sizeof(float2);
+      if ((e = dalloc(h, &h->fspec, sb))) { fail(e, "cudaMalloc spectrum"); break; }
+      if ((e = cudaMemsetAsync(h->fspec, 0, sb, h->st))) { fail(e, "memset"); break; }
+      if ((e = cudaMemsetAsync(h->fp0, 0, fb, h->st)) || (e = cudaMemsetAsync(h->fdp, 0, fb, h->st))) {
+        fail(e, "memset");
+        break;
+      }
+    }
     h->nparts = mhit::project_partials(n);
-    if ((e = dalloc(h, &h->partials, (size_t)h->nparts * 6 * sizeof(double)))) { fail(e, "cudaMalloc partials"); break; }
+    if ((e = dalloc(h, &h->partials, (size_t)h->nparts * 7 * sizeof(double)))) { fail(e, "cudaMalloc partials"); break; }
     if ((e = dalloc(h, &h->ctrl, sizeof(Ctrl)))) { fail(e, "cudaMalloc ctrl"); break; }
+    if ((e = dalloc(h, &h->stat_partials, (size_t)mhit::stats_partials(n) * 8 * sizeof(double))) ||
+        (e = dalloc(h, &h->stat_out, 8 * sizeof(double))) || (e = cudaMallocHost(&h->h_stat, 8 * sizeof(double)))) {
+      fail(e, "cudaMalloc stats");
+      break;
+    }
     if ((e = cudaMallocHost(&h->h_ctrl, sizeof(Ctrl)))) { fail(e, "cudaMallocHost"); break; }
     // tables: twiddles e^{-2 pi i m/n}, k^2, forcing sin/cos
     std::vector<double2> tw(n);
@@ -353,6 +523,17 @@ int mhit_create(const mhit_params* p, int nx, int ny, int nz, int precision, int
     for (int m = 0; m < n; ++m) {
       fs[m] = sin(p->k0 * x[m]);
       fc[m] = cos(p->k0 * x[m]);
+    }
+    std::vector<float2> twf(n);
+    for (int m = 0; m < n; ++m) {
+      long double a = 2.0L * 3.141592653589793238462643383279502884L * (long double)m / (long double)n;
+      twf[m].x = (float)cosl(a);
+      twf[m].y = -(float)sinl(a);
+    }
+    if ((e = dalloc(h, &h->ftw, n * sizeof(float2))) ||
+        (e = cudaMemcpyAsync(h->ftw, twf.data(), n * sizeof(float2), cudaMemcpyHostToDevice, h->st))) {
+      fail(e, "twiddles");
+      break;
     }
     if ((e = dalloc(h, &h->tw, n * sizeof(double2))) || (e = dalloc(h, &h->k2tab, n * sizeof(double))) ||
         (e = dalloc(h, &h->fsin, n * sizeof(double))) || (e = dalloc(h, &h->fcos, n * sizeof(double)))) {
@@ -394,16 +575,19 @@ int mhit_set_fields(mhit_handle* h, const double* u, const double* v, const doub
   if (!h || !u || !v || !w || !layout_ok(layout)) return MHIT_ERR_INVALID;
   if (h->phase_field && !phi) return MHIT_ERR_INVALID;
   DeviceGuard g(h->device);
-  const size_t fb = (size_t)h->n * h->n * h->n * sizeof(double);
-  CK(h, upload(h, h->u, u, layout));
-  CK(h, upload(h, h->v, v, layout));
-  CK(h, upload(h, h->w, w, layout));
-  if (h->phase_field) CK(h, upload(h, h->phi[0], phi, layout));
+  const size_t fb = (size_t)h->n * h->n * h->n * elem_size(h);
+  CK(h, put_field(h, fu(h), u, layout));
+  CK(h, put_field(h, fv(h), v, layout));
+  CK(h, put_field(h, fw(h), w, layout));
+  if (h->phase_field) CK(h, put_field(h, fphi(h, 0), phi, layout));
   // rhs_o starts at zero; beta = 0 on the first step (multi/main.f90:324)
-  CK(h, cudaMemsetAsync(h->ru, 0, fb, h->st));
-  CK(h, cudaMemsetAsync(h->rv, 0, fb, h->st));
-  CK(h, cudaMemsetAsync(h->rw, 0, fb, h->st));
-  CK(h, cudaMemsetAsync(h->p, 0, fb, h->st));
+  for (int q = 0; q < 3; ++q) CK(h, cudaMemsetAsync(frhs_o(h, q).ptr, 0, fb, h->st));
+  if (f32(h)) {
+    CK(h, cudaMemsetAsync(h->fp0, 0, fb, h->st));
+    CK(h, cudaMemsetAsync(h->fdp, 0, fb, h->st));
+  } else {
+    CK(h, cudaMemsetAsync(h->p, 0, fb, h->st));
+  }
   reset_ctrl(h);
   CK(h, cudaMemcpyAsync(h->ctrl, h->h_ctrl, sizeof(Ctrl), cudaMemcpyHostToDevice, h->st));
   CK(h, cudaStreamSynchronize(h->st));
@@ -415,7 +599,7 @@ int mhit_set_fields(mhit_handle* h, const double* u, const double* v, const doub
 int mhit_sync_state(mhit_handle* h) {
   if (!h) return MHIT_ERR_INVALID;
   DeviceGuard g(h->device);
-  CK(h, mhit::launch_materialize<double>(h->u, h->v, h->w, h->n, h->ctrl, h->st));
+  CK(h, materialize(h));
   return MHIT_OK;
 }
 
@@ -423,13 +607,13 @@ int mhit_get_fields(mhit_handle* h, double* u, double* v, double* w, double* phi
   if (!h || !layout_ok(layout)) return MHIT_ERR_INVALID;
   if (!h->has_fields) return MHIT_ERR_STATE;
   DeviceGuard g(h->device);
-  CK(h, mhit::launch_materialize<double>(h->u, h->v, h->w, h->n, h->ctrl, h->st));
+  CK(h, materialize(h));
   CK(h, pull_ctrl(h));
   const int cur = (int)(h->h_ctrl->nstep & 1);
-  if (u) CK(h, download(h, u, h->u, layout));
-  if (v) CK(h, download(h, v, h->v, layout));
-  if (w) CK(h, download(h, w, h->w, layout));
-  if (phi && h->phase_field) CK(h, download(h, phi, h->phi[cur], layout));
+  if (u) CK(h, get_field(h, u, fu(h), layout));
+  if (v) CK(h, get_field(h, v, fv(h), layout));
+  if (w) CK(h, get_field(h, w, fw(h), layout));
+  if (phi && h->phase_field) CK(h, get_field(h, phi, fphi(h, cur), layout));
   CK(h, cudaStreamSynchronize(h->st));
   if (layout == MHIT_LAYOUT_PIX_HALO) {
     double* outs[4] = {u, v, w, h->phase_field ? phi : nullptr};
@@ -439,11 +623,25 @@ int mhit_get_fields(mhit_handle* h, double* u, double* v, double* w, double* phi
   return MHIT_OK;
 }
 
+// The FP32 form's pressure is p0 + dp, summed in FP64 on the host.
 int mhit_get_pressure(mhit_handle* h, double* p, int layout) {
   if (!h || !p || !layout_ok(layout)) return MHIT_ERR_INVALID;
   DeviceGuard g(h->device);
-  CK(h, download(h, p, h->p, layout));
-  CK(h, cudaStreamSynchronize(h->st));
+  if (f32(h)) {
+    const size_t N3 = (size_t)h->n * h->n * h->n;
+    std::vector<double> a(N3), b(N3);
+    CK(h, get_field(h, a.data(), DevField{h->fp0, true}, MHIT_LAYOUT_RAW));
+    CK(h, get_field(h, b.data(), DevField{h->fdp, true}, MHIT_LAYOUT_RAW));
+    for (size_t q = 0; q < N3; ++q) a[q] += b[q];
+    const size_t plane = (size_t)h->n * h->n;
+    for (int k = 0; k < h->n; ++k) {
+      double* t = (layout == MHIT_LAYOUT_RAW) ? p + plane * k : p + (size_t)h->n * (1 + (size_t)(h->n + 2) * (k + 1));
+      memcpy(t, a.data() + plane * k, plane * sizeof(double));
+    }
+  } else {
+    CK(h, download(h, p, h->p, layout));
+    CK(h, cudaStreamSynchronize(h->st));
+  }
   if (layout == MHIT_LAYOUT_PIX_HALO) fill_halo_host(p, h->n);
   return MHIT_OK;
 }
@@ -487,17 +685,50 @@ int mhit_get_diag(mhit_handle* h, mhit_diag* out) {
   return MHIT_OK;
 }
 
+int mhit_diagnostics(mhit_handle* h, int pi_f32, mhit_stats* out) {
+  if (!h || !out) return MHIT_ERR_INVALID;
+  if (!h->has_fields) return MHIT_ERR_STATE;
+  DeviceGuard g(h->device);
+  CK(h, pull_ctrl(h));
+  const int n = h->n;
+  const int cur = (int)(h->h_ctrl->nstep & 1);
+  double dxi_d = h->c.dxi;
+  if (pi_f32) {
+    const double pi32 = (double)(float)3.14159265358979;  // post/compute_diss/module.f90:5
+    dxi_d = 1.0 / ((2 * pi32) / (n - 1));
+  }
+  if (f32(h))
+    CK(h, mhit::launch_stats<float>(h->fu, h->fv, h->fw, h->phase_field ? h->fphi[cur] : nullptr, h->ctrl, n,
+                                    h->c.dxi, dxi_d, h->stat_partials, h->stat_out, h->st));
+  else
+    CK(h, mhit::launch_stats<double>(h->u, h->v, h->w, h->phase_field ? h->phi[cur] : nullptr, h->ctrl, n,
+                                     h->c.dxi, dxi_d, h->stat_partials, h->stat_out, h->st));
+  CK(h, cudaMemcpyAsync(h->h_stat, h->stat_out, 8 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  CK(h, cudaStreamSynchronize(h->st));
+  const double nd = (double)n, n3 = nd * nd * nd;
+  const double* r = h->h_stat;
+  out->ke = 0.5 * r[0] / n3;
+  out->dissipation = 2 * (h->prm.mu / h->prm.rho) * r[1] / nd / nd / nd;
+  out->max_div = r[2];
+  out->phi_sum = h->phase_field ? r[3] : 0.0;
+  out->phi_min = h->phase_field ? r[4] : 0.0;
+  out->phi_max = h->phase_field ? r[5] : 0.0;
+  out->umean = r[6] / n3;
+  out->reserved = 0;
+  return MHIT_OK;
+}
+
 void* mhit_stream(mhit_handle* h) { return h ? (void*)h->st : nullptr; }
 
 int mhit_device_state(mhit_handle* h, void** u, void** v, void** w, void** phi) {
   if (!h) return MHIT_ERR_INVALID;
   DeviceGuard g(h->device);
-  if (u) *u = h->u;
-  if (v) *v = h->v;
-  if (w) *w = h->w;
+  if (u) *u = fu(h).ptr;
+  if (v) *v = fv(h).ptr;
+  if (w) *w = fw(h).ptr;
   if (phi) {
     CK(h, pull_ctrl(h));
-    *phi = h->phase_field ? (void*)h->phi[h->h_ctrl->nstep & 1] : nullptr;
+    *phi = h->phase_field ? fphi(h, (int)(h->h_ctrl->nstep & 1)).ptr : nullptr;
   }
   return MHIT_OK;
 }
@@ -510,46 +741,30 @@ int mhit_memory_bytes(mhit_handle* h, size_t* bytes) {
 
 int mhit_launches_per_step(mhit_handle* h, int* n) {
   if (!h || !n) return MHIT_ERR_INVALID;
-  *n = (h->phase_field ? 1 : 0) + 1 + 5 + 1 + 1;
+  *n = (int)step_stages(h, 0).size();
   return MHIT_OK;
 }
 
 // Run `reps` steps with every kernel launched on its own between CUDA events
-// on the handle's stream; ms[k] = mean duration of stage k.  Stage names in
-// launch order: phase (ACDI only), momentum, xfwd, yfwd, zsolve, yinv, xinv,
-// project, finalize.
-static const char* kStageNames[] = {"phase", "momentum", "xfwd", "yfwd", "zsolve", "yinv", "xinv", "project",
-                                    "finalize"};
-
+// on the handle's stream; ms[k] = mean duration of stage k (names from
+// mhit_stage_name, in launch order).
 int mhit_profile_step(mhit_handle* h, int reps, double* ms, int* nstages) {
   if (!h || !ms || !nstages || reps < 1) return MHIT_ERR_INVALID;
   if (!h->has_fields) return MHIT_ERR_STATE;
   DeviceGuard g(h->device);
-  const int NS = 9;
-  cudaEvent_t ev[NS + 1];
+  const int NS = (int)step_stages(h, 0).size();
+  std::vector<cudaEvent_t> ev(NS + 1);
   for (int i = 0; i <= NS; ++i) CK(h, cudaEventCreate(&ev[i]));
-  double acc[NS] = {0};
+  std::vector<double> acc(NS, 0.0);
   for (int r = 0; r < reps; ++r) {
     const int cur = (int)(h->nstep_host & 1);
-    mhit::StencilArgs<double> a = stencil_args(h, cur);
-    mhit::PoissonArgs<double> pa;
-    pa.us = h->us; pa.vs = h->vs; pa.ws = h->ws; pa.rhs = nullptr; pa.spec = h->spec; pa.p = h->p;
-    pa.tw = h->tw; pa.k2tab = h->k2tab; pa.ctrl = h->ctrl; pa.cdiv = h->c.cdiv;
+    std::vector<Stage> stages = step_stages(h, cur);
     CK(h, cudaEventRecord(ev[0], h->st));
-    if (h->phase_field) CK(h, mhit::launch_phase<double>(a, h->st));
-    CK(h, cudaEventRecord(ev[1], h->st));
-    if (h->phase_field) a.phi_in = h->phi[cur ^ 1];
-    CK(h, mhit::launch_momentum<double>(a, h->phase_field != 0, h->st));
-    CK(h, cudaEventRecord(ev[2], h->st));
-    for (int stage = 0; stage < 5; ++stage) {
-      CK(h, mhit::launch_poisson_stage<double>(h->n, pa, stage, h->st));
-      CK(h, cudaEventRecord(ev[3 + stage], h->st));
+    for (int i = 0; i < NS; ++i) {
+      CK(h, stages[i].second());
+      CK(h, cudaEventRecord(ev[i + 1], h->st));
     }
-    CK(h, mhit::launch_project<double>(a, h->st));
-    CK(h, cudaEventRecord(ev[8], h->st));
-    CK(h, mhit::launch_finalize(h->partials, h->nparts, h->ctrl, h->c, h->st));
-    CK(h, cudaEventRecord(ev[9], h->st));
-    CK(h, cudaEventSynchronize(ev[9]));
+    CK(h, cudaEventSynchronize(ev[NS]));
     for (int i = 0; i < NS; ++i) {
       float t = 0;
       CK(h, cudaEventElapsedTime(&t, ev[i], ev[i + 1]));
@@ -565,10 +780,15 @@ int mhit_profile_step(mhit_handle* h, int reps, double* ms, int* nstages) {
   return h->h_ctrl->status;
 }
 
-const char* mhit_stage_name(int k) { return (k >= 0 && k < 9) ? kStageNames[k] : ""; }
+const char* mhit_stage_name(mhit_handle* h, int k) {
+  if (!h) return "";
+  std::vector<Stage> st = step_stages(h, 0);
+  return (k >= 0 && k < (int)st.size()) ? st[k].first : "";
+}
 
 int mhit_poisson_device(mhit_handle* h, const double* rhs_dev, double* p_dev) {
   if (!h || !rhs_dev || !p_dev) return MHIT_ERR_INVALID;
+  if (f32(h)) return MHIT_ERR_UNSUPPORTED;  // the FP64 stand-alone solve needs the FP64 spectrum
   DeviceGuard g(h->device);
   mhit::PoissonArgs<double> pa;
   pa.us = pa.vs = pa.ws = nullptr;
@@ -579,12 +799,14 @@ int mhit_poisson_device(mhit_handle* h, const double* rhs_dev, double* p_dev) {
   pa.k2tab = h->k2tab;
   pa.ctrl = nullptr;
   pa.cdiv = h->c.cdiv;
+  pa.ddxi = h->c.ddxi;
   CK(h, mhit::launch_poisson<double>(h->n, pa, h->st));
   return MHIT_OK;
 }
 
 int mhit_poisson(mhit_handle* h, const double* rhs, double* p) {
   if (!h || !rhs || !p) return MHIT_ERR_INVALID;
+  if (f32(h)) return MHIT_ERR_UNSUPPORTED;
   DeviceGuard g(h->device);
   const size_t fb = (size_t)h->n * h->n * h->n * sizeof(double);
   CK(h, cudaMemcpyAsync(h->p, rhs, fb, cudaMemcpyHostToDevice, h->st));
@@ -641,16 +863,18 @@ int mhit_save(mhit_handle* h, const char* dir, int t) {
   double* host = buf.data();
   int rc;
   const char* names[3] = {"u", "v", "w"};
-  double* dev[3] = {h->u, h->v, h->w};
+  DevField dev[3] = {fu(h), fv(h), fw(h)};
   DeviceGuard g(h->device);
-  CK(h, mhit::launch_materialize<double>(h->u, h->v, h->w, h->n, h->ctrl, h->st));
+  CK(h, materialize(h));
   CK(h, pull_ctrl(h));
-  for (int f = 0; f < 3; ++f) {
-    CK(h, cudaMemcpy(host, dev[f], N3 * sizeof(double), cudaMemcpyDeviceToHost));
-    if ((rc = write_raw(fname(dir, names[f], t), host, N3))) return rc;
+  for (int q = 0; q < 3; ++q) {
+    CK(h, get_field(h, host, dev[q], MHIT_LAYOUT_RAW));
+    CK(h, cudaStreamSynchronize(h->st));
+    if ((rc = write_raw(fname(dir, names[q], t), host, N3))) return rc;
   }
   if (h->phase_field) {
-    CK(h, cudaMemcpy(host, h->phi[h->h_ctrl->nstep & 1], N3 * sizeof(double), cudaMemcpyDeviceToHost));
+    CK(h, get_field(h, host, fphi(h, (int)(h->h_ctrl->nstep & 1)), MHIT_LAYOUT_RAW));
+    CK(h, cudaStreamSynchronize(h->st));
     if ((rc = write_raw(fname(dir, "phi", t), host, N3))) return rc;
   }
   char b[64];
@@ -669,10 +893,12 @@ int mhit_save(mhit_handle* h, const char* dir, int t) {
   sc.beta = h->h_ctrl->beta;
   sc.cfl = h->h_ctrl->cfl;
   bool ok = fwrite(&sc, sizeof(sc), 1, f) == 1;
-  double* ro[3] = {h->ru, h->rv, h->rw};
   for (int q = 0; q < 3 && ok; ++q) {
-    if (cudaMemcpy(host, ro[q], N3 * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) ok = false;
-    else ok = fwrite(host, sizeof(double), N3, f) == N3;
+    if (get_field(h, host, frhs_o(h, q), MHIT_LAYOUT_RAW) != cudaSuccess ||
+        cudaStreamSynchronize(h->st) != cudaSuccess)
+      ok = false;
+    else
+      ok = fwrite(host, sizeof(double), N3, f) == N3;
   }
   fclose(f);
   return ok ? MHIT_OK : MHIT_ERR_IO;
@@ -699,17 +925,17 @@ int mhit_load(mhit_handle* h, const char* dir, int t) {
   if (!f) return MHIT_OK;  // reference restart: Euler first step, gumax = 1
   Sidecar sc;
   bool ok = fread(&sc, sizeof(sc), 1, f) == 1 && memcmp(sc.magic, "MHITSTA1", 8) == 0 && sc.n == h->n;
-  double* ro[3] = {h->ru, h->rv, h->rw};
   DeviceGuard g(h->device);
   for (int q = 0; q < 3 && ok; ++q) {
     ok = fread(bu.data(), sizeof(double), N3, f) == N3;
-    if (ok) ok = cudaMemcpy(ro[q], bu.data(), N3 * sizeof(double), cudaMemcpyHostToDevice) == cudaSuccess;
+    if (ok) ok = put_field(h, frhs_o(h, q), bu.data(), MHIT_LAYOUT_RAW) == cudaSuccess;
   }
   fclose(f);
   if (!ok) return MHIT_ERR_IO;
-  // phi was uploaded into phi[0]; keep the parity convention phi[nstep & 1]
+  CK(h, cudaStreamSynchronize(h->st));
+  // phi was uploaded into slot 0; keep the parity convention phi[nstep & 1]
   if (h->phase_field && (sc.nstep & 1))
-    CK(h, cudaMemcpyAsync(h->phi[1], h->phi[0], N3 * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
+    CK(h, cudaMemcpyAsync(fphi(h, 1).ptr, fphi(h, 0).ptr, N3 * elem_size(h), cudaMemcpyDeviceToDevice, h->st));
   Ctrl* c = h->h_ctrl;
   c->gumax = sc.gumax;
   c->alpha = sc.alpha;

@@ -15,6 +15,7 @@ struct Ctrl {
   double cfl;           // gumax*dt*dxi of the last step
   double cfl_limit;     // step error above this (7 in the reference)
   double last_mean[3];  // means removed by the last step
+  double max_div;       // max |div u| of the FP64 projection (FP32 refine form)
   long long nstep;      // steps taken
   int status;           // sticky MHIT_* error; kernels return early when set
   int pad_;

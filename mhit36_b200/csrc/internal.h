@@ -10,16 +10,18 @@
 namespace mhit {
 
 template <class T> struct PoissonArgs {
-  const T* us;  // divergence inputs (ustar, vstar, wstar) or nullptr
-  const T* vs;
-  const T* ws;
-  const T* rhs;  // explicit RHS (stand-alone solve) or nullptr
-  typename C2<T>::t* spec;
-  T* p;
-  const typename C2<T>::t* tw;
-  const double* k2tab;
-  const Ctrl* ctrl;
-  T cdiv;
+  const T* us = nullptr;  // divergence inputs (ustar, vstar, wstar) or nullptr
+  const T* vs = nullptr;
+  const T* ws = nullptr;
+  const T* rhs = nullptr;  // explicit RHS (stand-alone solve) or nullptr
+  typename C2<T>::t* spec = nullptr;
+  T* p = nullptr;
+  const typename C2<T>::t* tw = nullptr;
+  const double* k2tab = nullptr;
+  const Ctrl* ctrl = nullptr;
+  double cdiv = 0;         // rho*dxi/dt
+  const T* pres = nullptr;  // refinement: first-solve pressure p0 (residual RHS) or nullptr
+  double ddxi = 0;         // 1/dx^2 for the residual Laplacian
 };
 
 template <class T> cudaError_t launch_poisson(int n, const PoissonArgs<T>& a, cudaStream_t st);
@@ -40,7 +42,7 @@ template <class T> struct StencilArgs {
   T* ru;
   T* rv;
   T* rw;
-  const T* p;
+  const T* p;  // pressure (FP64 form) or first-solve p0 (FP32 refine)
   T* uo;
   T* vo;
   T* wo;
@@ -54,10 +56,19 @@ template <class T> struct StencilArgs {
 template <class T> cudaError_t launch_phase(const StencilArgs<T>& a, cudaStream_t st);
 template <class T> cudaError_t launch_momentum(const StencilArgs<T>& a, bool phase_field, cudaStream_t st);
 template <class T> cudaError_t launch_project(const StencilArgs<T>& a, cudaStream_t st);
-cudaError_t launch_finalize(const double* partials, int nparts, Ctrl* ctrl, StepConst c, cudaStream_t st);
+// FP32 refinement form: p = p0 + dp, projection and max|div u| in FP64.
+cudaError_t launch_project_refine(const StencilArgs<float>& a, const float* dp, cudaStream_t st);
+int project_refine_partials(int n);
+cudaError_t launch_finalize(const double* partials, int nparts, int stride, Ctrl* ctrl, StepConst c,
+                            cudaStream_t st);
 template <class T> cudaError_t launch_materialize(T* u, T* v, T* w, int n, Ctrl* ctrl, cudaStream_t st);
 cudaError_t prepare_stencils();
 int project_partials(int n);
 int stencil_size_ok(int n);
+
+template <class T>
+cudaError_t launch_stats(const T* u, const T* v, const T* w, const T* phi, const Ctrl* ctrl, int n, double dxi_c,
+                         double dxi_d, double* partials, double* out, cudaStream_t st);
+int stats_partials(int n);
 
 }  // namespace mhit

@@ -32,13 +32,41 @@ template <int N> struct PCfg {
 
 // ---------------------------------------------------------------- x forward
 // MODE 0: rhs = (rho*dxi/dt) * forward-difference divergence of (us,vs,ws)
-// (multi/main.f90:715-729).  MODE 1: rhs read from `rhs` (stand-alone solve).
+// (multi/main.f90:715-729), evaluated in FP64.
+// MODE 1: rhs read from `rhs` (stand-alone solve).
+// MODE 2: refinement residual r - L(p0) in FP64, r as in MODE 0 and L the
+// 7-point Laplacian (the operator whose symbol the FD-modified k^2 inverts).
+template <int N, int MODE, class T>
+__device__ __forceinline__ double xfwd_rhs(const T* __restrict__ us, const T* __restrict__ vs,
+                                          const T* __restrict__ ws, const T* __restrict__ rhs,
+                                          const T* __restrict__ p0, double cdiv, double ddxi, int n, int j,
+                                          int k) {
+  const size_t a = gidx(n, j, k, N);
+  if (MODE == 1) return (double)rhs[a];
+  const int ip = (n + 1 == N) ? 0 : n + 1;
+  const int jp = (j + 1 == N) ? 0 : j + 1;
+  const int kp = (k + 1 == N) ? 0 : k + 1;
+  double r = cdiv * ((double)us[gidx(ip, j, k, N)] - (double)us[a]);
+  r = r + cdiv * ((double)vs[gidx(n, jp, k, N)] - (double)vs[a]);
+  r = r + cdiv * ((double)ws[gidx(n, j, kp, N)] - (double)ws[a]);
+  if (MODE == 2) {
+    const int im = n ? n - 1 : N - 1, jm = j ? j - 1 : N - 1, km = k ? k - 1 : N - 1;
+    const double c = (double)p0[a];
+    const double lap = ((double)p0[gidx(ip, j, k, N)] - 2.0 * c + (double)p0[gidx(im, j, k, N)]) * ddxi +
+                       ((double)p0[gidx(n, jp, k, N)] - 2.0 * c + (double)p0[gidx(n, jm, k, N)]) * ddxi +
+                       ((double)p0[gidx(n, j, kp, N)] - 2.0 * c + (double)p0[gidx(n, j, km, N)]) * ddxi;
+    r = r - lap;
+  }
+  return r;
+}
+
 template <int N, int MODE, class T>
 __global__ void __launch_bounds__(256) xfwd_kernel(const T* __restrict__ us, const T* __restrict__ vs,
                                                   const T* __restrict__ ws, const T* __restrict__ rhs,
+                                                  const T* __restrict__ p0,
                                                   typename C2<T>::t* __restrict__ spec,
                                                   const typename C2<T>::t* __restrict__ tw,
-                                                  const Ctrl* __restrict__ ctrl, T cdiv) {
+                                                  const Ctrl* __restrict__ ctrl, double cdiv, double ddxi) {
   typedef typename C2<T>::t C;
   typedef PCfg<N> G;
   constexpr int P = G::P, NT = G::NT;
@@ -47,27 +75,12 @@ __global__ void __launch_bounds__(256) xfwd_kernel(const T* __restrict__ us, con
   C* s = reinterpret_cast<C*>(smem_raw);
   const int j0 = blockIdx.x * (2 * P);
   const int k = blockIdx.y;
-  const int kp = (k + 1 == N) ? 0 : k + 1;
   for (int wi = threadIdx.x; wi < P * N; wi += NT) {
     const int p = wi % P, n = wi / P;
-    const int ja = j0 + 2 * p, jb = ja + 1;
+    const int ja = j0 + 2 * p;
     C z;
-    if (MODE == 0) {
-      const int ip = (n + 1 == N) ? 0 : n + 1;
-      const int jbp = (jb + 1 == N) ? 0 : jb + 1;
-      const size_t a = gidx(n, ja, k, N), b = gidx(n, jb, k, N);
-      T ra = cdiv * (us[gidx(ip, ja, k, N)] - us[a]);
-      ra = ra + cdiv * (vs[b] - vs[a]);
-      ra = ra + cdiv * (ws[gidx(n, ja, kp, N)] - ws[a]);
-      T rb = cdiv * (us[gidx(ip, jb, k, N)] - us[b]);
-      rb = rb + cdiv * (vs[gidx(n, jbp, k, N)] - vs[b]);
-      rb = rb + cdiv * (ws[gidx(n, jb, kp, N)] - ws[b]);
-      z.x = ra;
-      z.y = rb;
-    } else {
-      z.x = rhs[gidx(n, ja, k, N)];
-      z.y = rhs[gidx(n, jb, k, N)];
-    }
+    z.x = (T)xfwd_rhs<N, MODE, T>(us, vs, ws, rhs, p0, cdiv, ddxi, n, ja, k);
+    z.y = (T)xfwd_rhs<N, MODE, T>(us, vs, ws, rhs, p0, cdiv, ddxi, n, ja + 1, k);
     s[n * P + p] = z;
   }
   __syncthreads();
@@ -217,6 +230,7 @@ template <int N, class T> static cudaError_t set_attrs() {
   const int xs = (int)xsmem<N, T>(), cs = (int)csmem<N, T>();
   if ((e = cudaFuncSetAttribute(xfwd_kernel<N, 0, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, xs))) return e;
   if ((e = cudaFuncSetAttribute(xfwd_kernel<N, 1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, xs))) return e;
+  if ((e = cudaFuncSetAttribute(xfwd_kernel<N, 2, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, xs))) return e;
   if ((e = cudaFuncSetAttribute(xinv_kernel<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, xs))) return e;
   if ((e = cudaFuncSetAttribute(ypass_kernel<N, -1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, cs))) return e;
   if ((e = cudaFuncSetAttribute(ypass_kernel<N, 1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, cs))) return e;
@@ -225,14 +239,27 @@ template <int N, class T> static cudaError_t set_attrs() {
 }
 
 template <int N, class T>
+static void launch_xfwd(const PoissonArgs<T>& a, cudaStream_t st) {
+  typedef PCfg<N> G;
+  const dim3 gx(N / (2 * G::P), N);
+  const size_t xs = xsmem<N, T>();
+  if (a.rhs)
+    xfwd_kernel<N, 1, T><<<gx, G::NT, xs, st>>>(nullptr, nullptr, nullptr, a.rhs, nullptr, a.spec, a.tw, a.ctrl,
+                                                a.cdiv, a.ddxi);
+  else if (a.pres)
+    xfwd_kernel<N, 2, T><<<gx, G::NT, xs, st>>>(a.us, a.vs, a.ws, nullptr, a.pres, a.spec, a.tw, a.ctrl, a.cdiv,
+                                                a.ddxi);
+  else
+    xfwd_kernel<N, 0, T><<<gx, G::NT, xs, st>>>(a.us, a.vs, a.ws, nullptr, nullptr, a.spec, a.tw, a.ctrl, a.cdiv,
+                                                a.ddxi);
+}
+
+template <int N, class T>
 static cudaError_t poisson_run(const PoissonArgs<T>& a, cudaStream_t st) {
   typedef PCfg<N> G;
   const dim3 gx(N / (2 * G::P), N), gc(G::NCHUNK, N);
   const size_t xs = xsmem<N, T>(), cs = csmem<N, T>();
-  if (a.rhs)
-    xfwd_kernel<N, 1, T><<<gx, G::NT, xs, st>>>(nullptr, nullptr, nullptr, a.rhs, a.spec, a.tw, a.ctrl, a.cdiv);
-  else
-    xfwd_kernel<N, 0, T><<<gx, G::NT, xs, st>>>(a.us, a.vs, a.ws, nullptr, a.spec, a.tw, a.ctrl, a.cdiv);
+  launch_xfwd<N, T>(a, st);
   ypass_kernel<N, -1, T><<<gc, G::NT, cs, st>>>(a.spec, a.tw, a.ctrl);
   zsolve_kernel<N, T><<<gc, G::NT, cs, st>>>(a.spec, a.tw, a.k2tab, a.ctrl);
   ypass_kernel<N, 1, T><<<gc, G::NT, cs, st>>>(a.spec, a.tw, a.ctrl);
@@ -246,12 +273,7 @@ static cudaError_t poisson_stage(const PoissonArgs<T>& a, int stage, cudaStream_
   const dim3 gx(N / (2 * G::P), N), gc(G::NCHUNK, N);
   const size_t xs = xsmem<N, T>(), cs = csmem<N, T>();
   switch (stage) {
-    case 0:
-      if (a.rhs)
-        xfwd_kernel<N, 1, T><<<gx, G::NT, xs, st>>>(nullptr, nullptr, nullptr, a.rhs, a.spec, a.tw, a.ctrl, a.cdiv);
-      else
-        xfwd_kernel<N, 0, T><<<gx, G::NT, xs, st>>>(a.us, a.vs, a.ws, nullptr, a.spec, a.tw, a.ctrl, a.cdiv);
-      break;
+    case 0: launch_xfwd<N, T>(a, st); break;
     case 1: ypass_kernel<N, -1, T><<<gc, G::NT, cs, st>>>(a.spec, a.tw, a.ctrl); break;
     case 2: zsolve_kernel<N, T><<<gc, G::NT, cs, st>>>(a.spec, a.tw, a.k2tab, a.ctrl); break;
     case 3: ypass_kernel<N, 1, T><<<gc, G::NT, cs, st>>>(a.spec, a.tw, a.ctrl); break;

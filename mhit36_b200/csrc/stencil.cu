@@ -350,6 +350,85 @@ __global__ void __launch_bounds__(NT) project_kernel(StencilArgs<T> a) {
   }
 }
 
+// ============================================================ projection (FP32 refine)
+// FP32 refinement form of C2 + R1: the pressure is p = p0 + dp (first FP32
+// solve plus the FP32 correction solve of the FP64 residual), the projection
+// u = ustar - dt/rho*(p - p_m)*dxi is evaluated in FP64 and rounded to FP32
+// only when stored, and the forward-difference divergence of the FP64
+// projected field is reduced (max |div u|) before that rounding.
+__global__ void __launch_bounds__(NT) project_refine_kernel(StencilArgs<float> a, const float* __restrict__ dp) {
+  if (a.ctrl->status) return;
+  const int n = a.c.n;
+  const double dtr = a.c.dtr, dxi = a.c.dxi;
+  const int i = blockIdx.x * TX + threadIdx.x % TX, j = blockIdx.y * TY + threadIdx.x / TX;
+  const int k0 = blockIdx.z * PKZ;
+  const int im = i ? i - 1 : n - 1, jm = j ? j - 1 : n - 1;
+  const int ip = (i + 1 == n) ? 0 : i + 1, jp = (j + 1 == n) ? 0 : j + 1;
+  const size_t nn = (size_t)n * n;
+  const float* p0 = a.p;
+  auto P = [&](size_t g) { return (double)p0[g] + (double)dp[g]; };
+  double su = 0, sv = 0, sw = 0, mdiv = 0;
+  double xu = -INFINITY, xv = -INFINITY, xw = -INFINITY;
+  const size_t col = (size_t)i + (size_t)n * j;
+  double pm = P(col + nn * wrapi(k0 - 1, n));
+  double pc = P(col + nn * k0);
+  double wsc = (double)a.ws[col + nn * k0];
+  for (int k = k0; k < k0 + PKZ; ++k) {
+    const size_t g = col + nn * k;
+    const int kp = (k + 1 == n) ? 0 : k + 1;
+    const size_t gzp = col + nn * kp;
+    const double pn = P(gzp);
+    const double wsn = (double)a.ws[gzp];
+    const size_t gxm = g - i + im, gxp = g - i + ip;
+    const size_t gym = g - (size_t)n * j + (size_t)n * jm, gyp = g - (size_t)n * j + (size_t)n * jp;
+    const double uo = (double)a.us[g] - dtr * (pc - P(gxm)) * dxi;
+    const double vo = (double)a.vs[g] - dtr * (pc - P(gym)) * dxi;
+    const double wo = wsc - dtr * (pc - pm) * dxi;
+    const double u1 = (double)a.us[gxp] - dtr * (P(gxp) - pc) * dxi;
+    const double v1 = (double)a.vs[gyp] - dtr * (P(gyp) - pc) * dxi;
+    const double w1 = wsn - dtr * (pn - pc) * dxi;
+    const double div = ((u1 - uo) + (v1 - vo) + (w1 - wo)) * dxi;
+    mdiv = fmax(mdiv, fabs(div));
+    if (div != div) mdiv = NAN;
+    a.uo[g] = (float)uo;
+    a.vo[g] = (float)vo;
+    a.wo[g] = (float)wo;
+    su += uo;
+    sv += vo;
+    sw += wo;
+    xu = fmax(xu, uo);
+    xv = fmax(xv, vo);
+    xw = fmax(xw, wo);
+    if (uo != uo || vo != vo || wo != wo) su = NAN;
+    pm = pc;
+    pc = pn;
+    wsc = wsn;
+  }
+  double vals[7] = {su, sv, sw, xu, xv, xw, mdiv};
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+    for (int t = 0; t < 3; ++t) vals[t] += __shfl_xor_sync(0xffffffffu, vals[t], o);
+#pragma unroll
+    for (int t = 3; t < 7; ++t) vals[t] = fmax(vals[t], __shfl_xor_sync(0xffffffffu, vals[t], o));
+  }
+  __shared__ double red[NT / 32][7];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0)
+    for (int t = 0; t < 7; ++t) red[wid][t] = vals[t];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double r[7];
+    for (int t = 0; t < 7; ++t) r[t] = red[0][t];
+    for (int w = 1; w < NT / 32; ++w) {
+      for (int t = 0; t < 3; ++t) r[t] += red[w][t];
+      for (int t = 3; t < 7; ++t) r[t] = fmax(r[t], red[w][t]);
+    }
+    const size_t b = (size_t)blockIdx.x + (size_t)gridDim.x * (blockIdx.y + (size_t)gridDim.y * blockIdx.z);
+    for (int t = 0; t < 7; ++t) a.partials[b * 7 + t] = r[t];
+  }
+}
+
 // ============================================================ finalize
 // M1, C3, R2 and the CFL guard (multi/main.f90:906-946), one CTA:
 // means = sum/nx/ny/nz, removed lazily (stored in ctrl->mean and subtracted by
@@ -358,23 +437,30 @@ __global__ void __launch_bounds__(NT) project_kernel(StencilArgs<T> a) {
 // monotonic; then gamma, CFL, AB2 switch and the sticky error status.
 constexpr int FNT = 1024;
 
-__global__ void __launch_bounds__(FNT) finalize_kernel(const double* __restrict__ partials, int nparts, Ctrl* ctrl,
-                                                       StepConst c) {
+// Partials hold `stride` values per CTA: sums of u, v, w, maxima of u, v, w,
+// and (stride 7, FP32 refine form) the max |div u| of the FP64 projection.
+__global__ void __launch_bounds__(FNT) finalize_kernel(const double* __restrict__ partials, int nparts, int stride,
+                                                       Ctrl* ctrl, StepConst c) {
   if (ctrl->status) return;
-  double v[6] = {0, 0, 0, -INFINITY, -INFINITY, -INFINITY};
+  double v[7] = {0, 0, 0, -INFINITY, -INFINITY, -INFINITY, 0};
   for (int b = threadIdx.x; b < nparts; b += FNT) {
-    for (int t = 0; t < 3; ++t) v[t] += partials[(size_t)b * 6 + t];
-    for (int t = 3; t < 6; ++t) v[t] = fmax(v[t], partials[(size_t)b * 6 + t]);
+    for (int t = 0; t < 3; ++t) v[t] += partials[(size_t)b * stride + t];
+    for (int t = 3; t < stride; ++t) v[t] = fmax(v[t], partials[(size_t)b * stride + t]);
   }
-  __shared__ double red[FNT][6];
-  for (int t = 0; t < 6; ++t) red[threadIdx.x][t] = v[t];
+  __shared__ double red[FNT / 32][7];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    for (int t = 0; t < 3; ++t) v[t] += __shfl_xor_sync(0xffffffffu, v[t], o);
+    for (int t = 3; t < 7; ++t) v[t] = fmax(v[t], __shfl_xor_sync(0xffffffffu, v[t], o));
+  }
+  if ((threadIdx.x & 31) == 0)
+    for (int t = 0; t < 7; ++t) red[threadIdx.x >> 5][t] = v[t];
   __syncthreads();
-  for (int s = FNT / 2; s > 0; s >>= 1) {
-    if (threadIdx.x < s) {
-      for (int t = 0; t < 3; ++t) red[threadIdx.x][t] += red[threadIdx.x + s][t];
-      for (int t = 3; t < 6; ++t) red[threadIdx.x][t] = fmax(red[threadIdx.x][t], red[threadIdx.x + s][t]);
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < FNT / 32; ++w) {
+      for (int t = 0; t < 3; ++t) red[0][t] += red[w][t];
+      for (int t = 3; t < 7; ++t) red[0][t] = fmax(red[0][t], red[w][t]);
     }
-    __syncthreads();
   }
   if (threadIdx.x == 0) {
     const double nd = (double)c.n;
@@ -394,6 +480,7 @@ __global__ void __launch_bounds__(FNT) finalize_kernel(const double* __restrict_
     ctrl->cfl = cou;
     ctrl->alpha = 1.5;
     ctrl->beta = 0.5;
+    ctrl->max_div = (stride > 6) ? red[0][6] : -1.0;
     ctrl->nstep += 1;
     const double s = red[0][0] + red[0][1] + red[0][2];
     if (!isfinite(s) || !isfinite(umax)) ctrl->status = 5;  // MHIT_ERR_NONFINITE
@@ -475,8 +562,18 @@ template <class T> cudaError_t launch_project(const StencilArgs<T>& a, cudaStrea
   return cudaGetLastError();
 }
 
-cudaError_t launch_finalize(const double* partials, int nparts, Ctrl* ctrl, StepConst c, cudaStream_t st) {
-  finalize_kernel<<<1, FNT, 0, st>>>(partials, nparts, ctrl, c);
+cudaError_t launch_project_refine(const StencilArgs<float>& a, const float* dp, cudaStream_t st) {
+  const int n = a.c.n;
+  dim3 grid(n / TX, n / TY, n / PKZ);
+  project_refine_kernel<<<grid, NT, 0, st>>>(a, dp);
+  return cudaGetLastError();
+}
+
+int project_refine_partials(int n) { return project_partials(n); }
+
+cudaError_t launch_finalize(const double* partials, int nparts, int stride, Ctrl* ctrl, StepConst c,
+                            cudaStream_t st) {
+  finalize_kernel<<<1, FNT, 0, st>>>(partials, nparts, stride, ctrl, c);
   return cudaGetLastError();
 }
 

@@ -14,7 +14,7 @@ import os
 import numpy as np
 
 from . import capi
-from .capi import MhitDiag, MhitError, MhitParams, load_library
+from .capi import MhitDiag, MhitError, MhitParams, MhitStats, load_library
 from .config import InputParams
 
 
@@ -138,6 +138,12 @@ class Solver:
         self._check(self.lib.mhit_get_diag(self.h, ctypes.byref(d)), "mhit_get_diag")
         return d.as_dict()
 
+    def stats(self, pi_f32: bool = True) -> dict:
+        """FP64 KE, dissipation (post/compute_diss convention), max|div u|, phi sum/bounds."""
+        st = MhitStats()
+        self._check(self.lib.mhit_diagnostics(self.h, int(pi_f32), ctypes.byref(st)), "mhit_diagnostics")
+        return st.as_dict()
+
     # -- files
     def save(self, outdir: str, t: int):
         os.makedirs(outdir, exist_ok=True)
@@ -183,10 +189,7 @@ class Solver:
         self._check(rc, "mhit_profile_step")
         out = {}
         for k in range(ns.value):
-            name = self.lib.mhit_stage_name(k).decode()
-            if name == "phase" and not self.phase_field:
-                continue
-            out[name] = ms[k]
+            out[self.lib.mhit_stage_name(self.h, k).decode()] = ms[k]
         return out
 
     def stream(self) -> int:

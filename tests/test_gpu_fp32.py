@@ -1,0 +1,106 @@
+"""GPU tests of the FP32 + FP64-residual refinement form and the FP64
+diagnostics, against the FP64 form on the same inputs.
+
+Both forms use the FD-modified k^2 here (the refinement needs a solve that
+inverts the 7-point Laplacian exactly).  Bars:
+  * max |div u| of the FP64 projection result <= 1e-10 every step;
+  * relative error of kinetic energy and dissipation vs the FP64 form <= 1e-4;
+  * velocity / phi within a few 1e-5 (relative to the field maximum).
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _params(**kw):
+    from mhit36_b200.config import InputParams
+    base = dict(dt=1e-3, mu=6e-3, rho=1.0, sigma=0.5, epsr=1.0, lin_force=0.1, k2_mode=1)
+    base.update(kw)
+    return InputParams(**base)
+
+
+def _case(n, pf=True):
+    from mhit36_b200 import fields
+    return fields.seeded_case(n, phase_field=pf, ndrops=4 if n <= 64 else None,
+                              rmin=0.4 if n <= 64 else None, rmax=0.6 if n <= 64 else None)
+
+
+def test_fp32_requires_fd_k2():
+    from mhit36_b200 import MhitError, Solver
+    from mhit36_b200.capi import MHIT_ERR_UNSUPPORTED
+    with pytest.raises(MhitError) as e:
+        Solver(32, _params(k2_mode=0), precision="fp32")
+    assert e.value.status == MHIT_ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("n,pf", [(64, True), (128, False)])
+def test_fp32_refine_vs_fp64(n, pf):
+    from mhit36_b200 import Solver
+    p = _params()
+    case = _case(n, pf)
+    steps = 50
+    with Solver(n, p, precision="fp64", phase_field=pf) as a, Solver(n, p, precision="fp32", phase_field=pf) as b:
+        a.set_fields(*case)
+        b.set_fields(*case)
+        worst_div = 0.0
+        for _ in range(steps):
+            a.step(1)
+            d = b.step(1)
+            worst_div = max(worst_div, d["max_div"])
+        ra, rb = a.get_fields(), b.get_fields()
+        sa, sb = a.stats(), b.stats()
+    assert worst_div <= 1e-10, worst_div
+    for x, y in zip(rb[:3], ra[:3]):
+        assert rel_err(x, y) < 5e-5
+    if pf:
+        assert rel_err(rb[3], ra[3]) < 5e-5
+    assert abs(sb["ke"] / sa["ke"] - 1) < 1e-4
+    assert abs(sb["dissipation"] / sa["dissipation"] - 1) < 1e-4
+
+
+def test_fp64_form_reports_no_div():
+    from mhit36_b200 import Solver
+    with Solver(32, _params(), phase_field=False) as s:
+        s.set_fields(*_case(32, False))
+        assert s.step(1)["max_div"] == -1.0
+
+
+def test_stats_match_oracle_dissipation():
+    """GPU dissipation (post/compute_diss convention) equals the oracle's."""
+    from oracle import dissipation
+    from mhit36_b200 import Solver, fields
+    from mhit36_b200.config import InputParams
+    n = 64
+    u, v, w = fields.taylor_green(n)
+    with Solver(n, InputParams(dt=2e-4, mu=6.25e-4, rho=1.0), phase_field=False) as s:
+        s.set_fields(u, v, w)
+        st0 = s.stats(pi_f32=True)
+        s.step(10)
+        uu, vv, ww, _ = s.get_fields()
+        st = s.stats(pi_f32=True)
+    assert abs(st0["dissipation"] / dissipation(u, v, w, 6.25e-4, True) - 1) < 1e-13
+    assert abs(st["dissipation"] / dissipation(uu, vv, ww, 6.25e-4, True) - 1) < 1e-13
+    ke = 0.5 * np.mean(uu ** 2 + vv ** 2 + ww ** 2)
+    assert abs(st["ke"] / ke - 1) < 1e-13
+
+
+def test_fp32_save_load_roundtrip(tmp_path):
+    from mhit36_b200 import Solver
+    n = 32
+    p = _params()
+    case = _case(n)
+    with Solver(n, p, precision="fp32") as a:
+        a.set_fields(*case)
+        a.step(3)
+        a.save(str(tmp_path), 3)
+        a.step(2)
+        ref = a.get_fields()
+    with Solver(n, p, precision="fp32") as b:
+        b.load(str(tmp_path), 3)
+        b.step(2)
+        got = b.get_fields()
+    for x, y in zip(ref, got):
+        assert np.array_equal(x, y)

@@ -221,3 +221,21 @@ def test_phi_volume_conserved_and_bounded():
         phi = s.get_fields()[3]
     assert abs(phi.sum() / case[3].sum() - 1) < 1e-11
     assert phi.min() > -0.05 and phi.max() < 1.05
+
+
+def test_ns_acdi_256_3_steps():
+    """256^3 NS+ACDI (8 drops) against the oracle: exercises the 8x8x4 radix plan."""
+    p = _params()
+    ref, got, od, d, _, _ = run_pair(256, 3, True, p)
+    _check(ref, got, True)
+
+
+@pytest.mark.parametrize("n", [256, 512])
+def test_poisson_manufactured_large(n):
+    """sin(x)cos(2y)sin(3z) at 256^3 and 512^3 (radix plans 8x8x4 and 8x8x8)."""
+    from mhit36_b200 import Solver
+    with Solver(n, _params(grid_mode=1), phase_field=False) as s:
+        x = np.arange(n) * (2 * np.pi / n)
+        p = np.sin(x)[:, None, None] * np.cos(2 * x)[None, :, None] * np.sin(3 * x)[None, None, :]
+        got = s.poisson(-14.0 * p)
+    assert np.max(np.abs(got - p)) < 1e-12
