@@ -30,8 +30,8 @@ module mhit_iface
     real(c_double) :: lin_force
     integer(c_int32_t) :: k2_mode, grid_mode
     real(c_double) :: cfl_limit
-    integer(c_int32_t) :: tanh_identity
-    integer(c_int32_t) :: reserved(7)
+    integer(c_int32_t) :: tanh_identity, phi_floor
+    integer(c_int32_t) :: reserved(6)
   end type mhit_params
 
   type, bind(C) :: mhit_diag

@@ -70,8 +70,11 @@ typedef struct mhit_params {
   int32_t k2_mode;                     /* MHIT_K2_* */
   int32_t grid_mode;                   /* MHIT_GRID_* */
   double cfl_limit;                    /* 7.0 in the reference (multi/main.f90:945) */
-  int32_t tanh_identity;               /* 1: tanh(psi/2eps) = (2phi-1)/(1+2enum); 0 = reference tanh */
-  int32_t reserved[7];
+  int32_t tanh_identity;               /* 1 (default): tanh(psi/(2eps)) evaluated as (2phi-1)/(1+2enum), its
+                                          exact value; 0: the FP64 tanh of multi/main.f90:463-465 */
+  int32_t phi_floor;                   /* 1 (default): psi from max(min(phi,1),0); 0: min(phi,1) only, as
+                                          multi/main.f90:388, which makes psi NaN once phi < -1e-16 */
+  int32_t reserved[6];
 } mhit_params;
 
 /* Per-step scalars (the values the reference prints or reduces). */
@@ -213,6 +216,7 @@ int mhit_step_async(mhit_handle* h, int nsteps);
 /* The handle's CUDA stream (cudaStream_t) and the last CUDA error text. */
 void* mhit_stream(mhit_handle* h);
 const char* mhit_last_error(mhit_handle* h);
+
 
 /* Free everything (multi/main.f90:979-985). */
 int mhit_destroy(mhit_handle* h);

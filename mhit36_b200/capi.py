@@ -40,7 +40,8 @@ class MhitParams(ctypes.Structure):
         ("k2_mode", ctypes.c_int32), ("grid_mode", ctypes.c_int32),
         ("cfl_limit", ctypes.c_double),
         ("tanh_identity", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 7),
+        ("phi_floor", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 6),
     ]
 
 

@@ -57,7 +57,8 @@ class InputParams:
     k2_mode: int = 0         # 0 spectral k^2 (reference), 1 FD-modified
     grid_mode: int = 0       # 0 dx = 2pi/(N-1) (reference), 1 dx = 2pi/N
     cfl_limit: float = 7.0   # multi/main.f90:945
-    tanh_identity: int = 0   # 1: tanh(psi/2eps) from phi directly
+    tanh_identity: int = 1   # 1: tanh(psi/2eps) as (2phi-1)/(1+2enum), its exact value; 0: FP64 tanh
+    phi_floor: int = 1       # 1: psi from max(min(phi,1),0); 0: min(phi,1) as the reference
 
     # derived constants, multi/readinput.f90:34-43
     def derived(self, n: int) -> dict:

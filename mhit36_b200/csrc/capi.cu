@@ -382,7 +382,8 @@ void mhit_default_params(mhit_params* p) {
   p->k2_mode = MHIT_K2_SPECTRAL;
   p->grid_mode = MHIT_GRID_REFERENCE;
   p->cfl_limit = 7.0;
-  p->tanh_identity = 0;
+  p->tanh_identity = 1;
+  p->phi_floor = 1;
 }
 
 int mhit_size_supported(int n) { return size_supported(n) ? 1 : 0; }
@@ -442,6 +443,7 @@ int mhit_create(const mhit_params* p, int nx, int ny, int nz, int precision, int
   c.f1 = p->f1; c.f2 = p->f2; c.f3 = p->f3;
   c.abc = (p->f1 != 0.0 || p->f2 != 0.0 || p->f3 != 0.0) ? 1 : 0;
   c.tanh_identity = p->tanh_identity ? 1 : 0;
+  c.phi_floor = p->phi_floor ? 1 : 0;
   c.cdiv = p->rho * c.dxi / p->dt;
   c.dtr = p->dt / p->rho;
 

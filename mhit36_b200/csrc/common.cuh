@@ -26,7 +26,7 @@ struct StepConst {
   int n;
   int abc;            // ABC forcing active
   int tanh_identity;  // tanh(psi/2eps) from phi directly
-  int pad_;
+  int phi_floor;      // psi from max(min(phi,1),0) instead of min(phi,1)
   double dt, mu, rho, rhoi, dxi, ddxi, eps, epsi, enumv, tiny, sigma, lin_force;
   double f1, f2, f3;
   double cdiv;        // rho*dxi/dt   (multi/main.f90:723)
@@ -37,6 +37,19 @@ __device__ __forceinline__ int wrapi(int a, int n) { return a < 0 ? a + n : (a >
 
 __device__ __forceinline__ size_t gidx(int i, int j, int k, int n) {
   return (size_t)i + (size_t)n * ((size_t)j + (size_t)n * (size_t)k);
+}
+
+// ---- asynchronous global -> shared copies (sm_80+ cp.async) ----
+// One element per call (4 or 8 bytes); a thread's copies land in issue
+// order groups: commit after a batch, wait until at most N groups are pending.
+template <class T> __device__ __forceinline__ void cp_async_elem(T* smem_dst, const T* gmem_src) {
+  static_assert(sizeof(T) == 4 || sizeof(T) == 8, "cp.async element size");
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gmem_src), "n"(sizeof(T)) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
 // ---- complex helpers (double2 / float2) ----

@@ -23,8 +23,12 @@
 namespace mhit {
 
 template <int N> struct PCfg {
-  static constexpr int P = (N >= 1024) ? 4 : 8;   // line pairs per CTA (x passes)
-  static constexpr int CC = (N >= 1024) ? 4 : 8;  // kx columns per CTA (y/z passes)
+  // Lines per CTA: 2048/N (at most 8), so that the first radix-8 stage gives
+  // every one of the 256 threads exactly one butterfly (registers stay under
+  // the 85 that three resident CTAs per SM allow).
+  static constexpr int L = (N <= 256) ? 8 : ((N <= 512) ? 4 : 2);
+  static constexpr int P = L;   // line pairs per CTA (x passes)
+  static constexpr int CC = L;  // kx columns per CTA (y/z passes)
   static constexpr int NT = 256;
   static constexpr int PITCH = ((N / 2 + 1) + CC - 1) / CC * CC;
   static constexpr int NCHUNK = PITCH / CC;
@@ -61,7 +65,7 @@ __device__ __forceinline__ double xfwd_rhs(const T* __restrict__ us, const T* __
 }
 
 template <int N, int MODE, class T>
-__global__ void __launch_bounds__(256) xfwd_kernel(const T* __restrict__ us, const T* __restrict__ vs,
+__global__ void __launch_bounds__(256, 3) xfwd_kernel(const T* __restrict__ us, const T* __restrict__ vs,
                                                   const T* __restrict__ ws, const T* __restrict__ rhs,
                                                   const T* __restrict__ p0,
                                                   typename C2<T>::t* __restrict__ spec,
@@ -104,7 +108,7 @@ __global__ void __launch_bounds__(256) xfwd_kernel(const T* __restrict__ us, con
 
 // ---------------------------------------------------------------- y pass
 template <int N, int DIR, class T>
-__global__ void __launch_bounds__(256) ypass_kernel(typename C2<T>::t* __restrict__ spec,
+__global__ void __launch_bounds__(256, 3) ypass_kernel(typename C2<T>::t* __restrict__ spec,
                                                    const typename C2<T>::t* __restrict__ tw,
                                                    const Ctrl* __restrict__ ctrl) {
   typedef typename C2<T>::t C;
@@ -131,7 +135,7 @@ __global__ void __launch_bounds__(256) ypass_kernel(typename C2<T>::t* __restric
 // (multi/main.f90:785-798), inverse z FFT, all in shared memory.
 // k2tab[m] holds kx(m)^2 (spectral) or (4/dx^2) sin^2(pi m/N) (FD-modified).
 template <int N, class T>
-__global__ void __launch_bounds__(256) zsolve_kernel(typename C2<T>::t* __restrict__ spec,
+__global__ void __launch_bounds__(256, 3) zsolve_kernel(typename C2<T>::t* __restrict__ spec,
                                                     const typename C2<T>::t* __restrict__ tw,
                                                     const double* __restrict__ k2tab,
                                                     const Ctrl* __restrict__ ctrl) {
@@ -179,7 +183,7 @@ __global__ void __launch_bounds__(256) zsolve_kernel(typename C2<T>::t* __restri
 // Complex-to-real x transform of two lines at once; writes p
 // (multi/main.f90:812, 842-850: p = real(psi)).
 template <int N, class T>
-__global__ void __launch_bounds__(256) xinv_kernel(const typename C2<T>::t* __restrict__ spec, T* __restrict__ p,
+__global__ void __launch_bounds__(256, 3) xinv_kernel(const typename C2<T>::t* __restrict__ spec, T* __restrict__ p,
                                                   const typename C2<T>::t* __restrict__ tw,
                                                   const Ctrl* __restrict__ ctrl) {
   typedef typename C2<T>::t C;

@@ -34,9 +34,13 @@ static int pick_kz(int n) { return n >= 32 ? 32 : n; }
 //   phi_new = phi + dt*rhs                                    (A7)
 // psi needs phi on a radius-2 neighbourhood; it is computed per plane on the
 // tile plus a 2-cell ring, F on the tile plus a 1-cell ring.
+constexpr int PTY = 16;            // phase tile height
+constexpr int PNT = TX * PTY;       // phase threads per CTA
+
 template <class T>
-__global__ void __launch_bounds__(NT) phase_kernel(StencilArgs<T> a, int KZ) {
+__global__ void __launch_bounds__(PNT, 2) phase_kernel(StencilArgs<T> a, int KZ) {
   if (a.ctrl->status) return;
+  constexpr int TY = PTY, NT = PNT;
   constexpr int EX = TX + 4, EY = TY + 4, PE = EX * EY;
   constexpr int FX = TX + 2, FY = TY + 2, FE = FX * FY;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -49,24 +53,37 @@ __global__ void __launch_bounds__(NT) phase_kernel(StencilArgs<T> a, int KZ) {
   const T gamma = (T)(1.0 * a.ctrl->gumax);  // multi/main.f90:362
   const T mu = (T)a.ctrl->mean[0], mv = (T)a.ctrl->mean[1], mw = (T)a.ctrl->mean[2];
   const int use_ident = a.c.tanh_identity;
+  const T floor0 = a.c.phi_floor ? (T)0 : (T)-INFINITY;
+  const T inv12e = (T)1 / ((T)1 + (T)2 * enumv);
   const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, k0 = blockIdx.z * KZ;
   const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
   const int i = x0 + tx, j = y0 + ty;
   const int ip = (i + 1 == n) ? 0 : i + 1, jp = (j + 1 == n) ? 0 : j + 1;
   const size_t nn = (size_t)n * n;
 
+  // phi plane m (2-cell ring) is copied into ring slot (m+15)%5 with
+  // cp.async one iteration ahead of its use.
+  auto issue = [&](int m) {
+    T* Pphi = s_phi + ((m + 15) % 5) * PE;
+    const T* src = a.phi_in + (size_t)wrapi(m, n) * nn;
+    for (int e = tid; e < PE; e += NT) {
+      const int ex = e % EX, ey = e / EX;
+      cp_async_elem(Pphi + e, src + (size_t)wrapi(x0 - 2 + ex, n) + (size_t)n * wrapi(y0 - 2 + ey, n));
+    }
+    cp_async_commit();
+  };
+  issue(k0 - 2);
   for (int m = k0 - 2; m <= k0 + KZ + 1; ++m) {
-    // (1) phi plane m on the tile + 2 ring, and psi there.
+    __syncthreads();  // every thread is done with the slots plane m+1 reuses
+    if (m + 1 <= k0 + KZ + 1) issue(m + 1);
+    else cp_async_commit();
+    cp_async_wait<1>();  // this thread's copies of plane m have landed
+    // (1) psi of plane m on the elements this thread copied.
     {
-      T* Pphi = s_phi + ((m + 15) % 5) * PE;
+      const T* Pphi = s_phi + ((m + 15) % 5) * PE;
       T* Ppsi = s_psi + ((m + 15) % 3) * PE;
-      const T* src = a.phi_in + (size_t)wrapi(m, n) * nn;
       for (int e = tid; e < PE; e += NT) {
-        const int ex = e % EX, ey = e / EX;
-        const int gx = wrapi(x0 - 2 + ex, n), gy = wrapi(y0 - 2 + ey, n);
-        const T f = src[gx + (size_t)n * gy];
-        Pphi[e] = f;
-        const T val = fmin(f, (T)1);
+        const T val = fmax(fmin(Pphi[e], (T)1), floor0);
         Ppsi[e] = eps * log((val + enumv) / ((T)1 - val + enumv));
       }
     }
@@ -88,8 +105,9 @@ __global__ void __launch_bounds__(NT) phase_kernel(StencilArgs<T> a, int KZ) {
         const T normod = (T)1 / (sqrt(gxv * gxv + gyv * gyv + gzv * gzv) + tiny);
         T t;
         if (use_ident) {
-          const T val = fmin(Phc[pe], (T)1);
-          t = ((T)2 * val - (T)1) / ((T)1 + (T)2 * enumv);
+          // tanh(0.5*log(a/b)) = (a-b)/(a+b) with a = val+enum, b = 1-val+enum
+          const T val = fmax(fmin(Phc[pe], (T)1), floor0);
+          t = ((T)2 * val - (T)1) * inv12e;
         } else {
           t = tanh((T)0.5 * Pc[pe] * epsi);
         }
@@ -160,27 +178,41 @@ __global__ void __launch_bounds__(NT) momentum_kernel(StencilArgs<T> a, int KZ) 
   const size_t nn = (size_t)n * n;
   const T h = (T)0.5, q = (T)0.25;
 
-  for (int m = k0 - 2; m <= k0 + KZ; ++m) {
-    const int mz = wrapi(m, n);
-    {
-      const int sl = (m + 8) & 3;
-      T* Su = s_u + sl * UE;
-      T* Sv = s_v + sl * UE;
-      T* Sw = s_w + sl * UE;
-      const size_t zoff = (size_t)mz * nn;
-      for (int e = tid; e < UE; e += NT) {
-        const int ex = e % UX, ey = e / UX;
-        const size_t gg = zoff + (size_t)wrapi(x0 - 1 + ex, n) + (size_t)n * wrapi(y0 - 1 + ey, n);
-        Su[e] = a.u[gg] - mu;
-        Sv[e] = a.v[gg] - mv;
-        Sw[e] = a.w[gg] - mw;
+  // Plane m of u, v, w (1-cell ring) and phi (2-cell ring) is copied into
+  // ring slot (m+8)&3 with cp.async one iteration ahead of its use, so the
+  // HBM latency of plane m+1 overlaps the arithmetic of plane m-1.
+  auto issue = [&](int m) {
+    const int sl = (m + 8) & 3;
+    const size_t zoff = (size_t)wrapi(m, n) * nn;
+    for (int e = tid; e < UE; e += NT) {
+      const int ex = e % UX, ey = e / UX;
+      const size_t gg = zoff + (size_t)wrapi(x0 - 1 + ex, n) + (size_t)n * wrapi(y0 - 1 + ey, n);
+      cp_async_elem(s_u + sl * UE + e, a.u + gg);
+      cp_async_elem(s_v + sl * UE + e, a.v + gg);
+      cp_async_elem(s_w + sl * UE + e, a.w + gg);
+    }
+    if (PF) {
+      for (int e = tid; e < PE; e += NT) {
+        const int ex = e % EX, ey = e / EX;
+        cp_async_elem(s_phi + sl * PE + e,
+                      a.phi_in + zoff + (size_t)wrapi(x0 - 2 + ex, n) + (size_t)n * wrapi(y0 - 2 + ey, n));
       }
-      if (PF) {
-        T* Sp = s_phi + sl * PE;
-        for (int e = tid; e < PE; e += NT) {
-          const int ex = e % EX, ey = e / EX;
-          Sp[e] = a.phi_in[zoff + (size_t)wrapi(x0 - 2 + ex, n) + (size_t)n * wrapi(y0 - 2 + ey, n)];
-        }
+    }
+    cp_async_commit();
+  };
+  issue(k0 - 2);
+  for (int m = k0 - 2; m <= k0 + KZ; ++m) {
+    __syncthreads();  // every thread is done with the slot plane m+1 reuses
+    if (m + 1 <= k0 + KZ) issue(m + 1);
+    else cp_async_commit();
+    cp_async_wait<1>();  // this thread's copies of plane m have landed
+    {
+      // the pending mean removal, on the elements this thread copied
+      const int sl = (m + 8) & 3;
+      for (int e = tid; e < UE; e += NT) {
+        s_u[sl * UE + e] -= mu;
+        s_v[sl * UE + e] -= mv;
+        s_w[sl * UE + e] -= mw;
       }
     }
     __syncthreads();
@@ -291,7 +323,7 @@ __global__ void __launch_bounds__(NT) momentum_kernel(StencilArgs<T> a, int KZ) 
 constexpr int PKZ = 16;
 
 template <class T>
-__global__ void __launch_bounds__(NT) project_kernel(StencilArgs<T> a) {
+__global__ void __launch_bounds__(NT, 4) project_kernel(StencilArgs<T> a) {
   if (a.ctrl->status) return;
   const int n = a.c.n;
   const T dtr = (T)a.c.dtr, dxi = (T)a.c.dxi;
@@ -507,7 +539,7 @@ __global__ void clear_mean_kernel(Ctrl* ctrl) {
 
 // ============================================================ launchers
 template <class T> static size_t phase_smem() {
-  return sizeof(T) * (size_t)(8 * (TX + 4) * (TY + 4) + 9 * (TX + 2) * (TY + 2));
+  return sizeof(T) * (size_t)(8 * (TX + 4) * (PTY + 4) + 9 * (TX + 2) * (PTY + 2));
 }
 template <class T> static size_t momentum_smem(bool pf) {
   size_t s = 3 * 4 * (TX + 2) * (TY + 2);
@@ -515,7 +547,9 @@ template <class T> static size_t momentum_smem(bool pf) {
   return sizeof(T) * s;
 }
 
-int stencil_size_ok(int n) { return n >= 32 && n % TX == 0 && n % TY == 0 && n % PKZ == 0 && n % pick_kz(n) == 0; }
+int stencil_size_ok(int n) {
+  return n >= 32 && n % TX == 0 && n % TY == 0 && n % PTY == 0 && n % PKZ == 0 && n % pick_kz(n) == 0;
+}
 
 int project_partials(int n) { return (n / TX) * (n / TY) * (n / PKZ); }
 
@@ -540,8 +574,8 @@ cudaError_t prepare_stencils() {
 
 template <class T> cudaError_t launch_phase(const StencilArgs<T>& a, cudaStream_t st) {
   const int n = a.c.n, kz = pick_kz(n);
-  dim3 grid(n / TX, n / TY, n / kz);
-  phase_kernel<T><<<grid, NT, phase_smem<T>(), st>>>(a, kz);
+  dim3 grid(n / TX, n / PTY, n / kz);
+  phase_kernel<T><<<grid, PNT, phase_smem<T>(), st>>>(a, kz);
   return cudaGetLastError();
 }
 

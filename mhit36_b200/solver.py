@@ -29,6 +29,7 @@ def make_params(p: InputParams) -> MhitParams:
     m.k2_mode = int(p.k2_mode)
     m.grid_mode = int(p.grid_mode)
     m.tanh_identity = int(p.tanh_identity)
+    m.phi_floor = int(p.phi_floor)
     return m
 
 

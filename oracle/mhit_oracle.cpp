@@ -58,6 +58,7 @@ typedef struct oracle_params {
   int grid_mode;      // 0 reference dx=2pi/(N-1), 1 consistent dx=2pi/N
   int phase_field;    // 1 = ACDI on (#define phiflag 1, multi/main.f90:39)
   int tanh_identity;  // 1 = use tanh(psi/2eps)=(2phi-1)/(1+2enum) (not the reference)
+  int phi_floor;      // 1 = psi from max(min(phi,1),0) (not the reference)
 } oracle_params;
 
 typedef struct oracle_diag {
@@ -222,7 +223,8 @@ struct Oracle {
     // A3: psi on all cells including halos (multi/main.f90:384-393)
 #pragma omp parallel for
     for (size_t n = 0; n < ntot; ++n) {
-      const double val = std::min(phi[n], 1.0);
+      double val = std::min(phi[n], 1.0);
+      if (prm.phi_floor) val = std::max(val, 0.0);
       psidi[n] = eps * std::log((val + enum_) / (1.0 - val + enum_));
     }
     // A4: raw gradient of psi (multi/main.f90:397-415)
@@ -252,8 +254,9 @@ struct Oracle {
     auto g = [&](size_t n) -> double {
       double t;
       if (prm.tanh_identity) {
-        const double val = std::min(phi[n], 1.0);
-        t = (2.0 * val - 1.0) / (1.0 + 2.0 * enum_);
+        double val = std::min(phi[n], 1.0);
+        if (prm.phi_floor) val = std::max(val, 0.0);
+        t = (2.0 * val - 1.0) * (1.0 / (1.0 + 2.0 * enum_));
       } else {
         t = std::tanh(0.5 * psidi[n] * epsi);
       }

@@ -34,6 +34,7 @@ class OracleParams(ctypes.Structure):
         ("grid_mode", ctypes.c_int),
         ("phase_field", ctypes.c_int),
         ("tanh_identity", ctypes.c_int),
+        ("phi_floor", ctypes.c_int),
     ]
 
 
@@ -106,13 +107,13 @@ class Oracle:
 
     def __init__(self, n: int, dt=1e-3, mu=6e-3, rho=1.0, f1=0.0, f2=0.0, f3=0.0, k0=2.0,
                  radius=0.5, sigma=0.5, epsr=1.0, lin_force=0.0, k2_mode=0, grid_mode=0,
-                 phase_field=1, tanh_identity=0, threads: int = 0):
+                 phase_field=1, tanh_identity=0, phi_floor=0, threads: int = 0):
         self.lib = _load()
         if threads:
             self.lib.oracle_set_threads(threads)
         self.n = n
         self.params = OracleParams(dt, mu, rho, f1, f2, f3, k0, radius, sigma, epsr, lin_force,
-                                   k2_mode, grid_mode, phase_field, tanh_identity)
+                                   k2_mode, grid_mode, phase_field, tanh_identity, phi_floor)
         self.h = self.lib.oracle_create(ctypes.byref(self.params), n)
         if not self.h:
             raise ValueError(f"oracle_create failed for n={n}")

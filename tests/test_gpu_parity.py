@@ -28,7 +28,7 @@ def _params(**kw):
 def _oracle_kw(p):
     return dict(dt=p.dt, mu=p.mu, rho=p.rho, f1=p.f1, f2=p.f2, f3=p.f3, k0=p.k0, radius=p.radius,
                 sigma=p.sigma, epsr=p.epsr, lin_force=p.lin_force, k2_mode=p.k2_mode, grid_mode=p.grid_mode,
-                tanh_identity=p.tanh_identity)
+                tanh_identity=p.tanh_identity, phi_floor=p.phi_floor)
 
 
 def _case(n, pf, ndrops=None, rmin=None, rmax=None, grid_mode=0):
@@ -36,11 +36,11 @@ def _case(n, pf, ndrops=None, rmin=None, rmax=None, grid_mode=0):
     return fields.seeded_case(n, phase_field=pf, ndrops=ndrops, rmin=rmin, rmax=rmax, grid_mode=grid_mode)
 
 
-def run_pair(n, steps, pf, p, case=None):
+def run_pair(n, steps, pf, p, case=None, oracle_p=None):
     from oracle import Oracle
     from mhit36_b200 import Solver
     u, v, w, phi = case if case is not None else _case(n, pf, grid_mode=p.grid_mode)
-    o = Oracle(n, phase_field=int(pf), **_oracle_kw(p))
+    o = Oracle(n, phase_field=int(pf), **_oracle_kw(oracle_p or p))
     o.set_fields(u, v, w, phi)
     rc, od = o.step(steps)
     assert rc == 0
@@ -88,10 +88,22 @@ def test_ns_acdi_128_10_steps():
     _check(ref, got, True)
 
 
-@pytest.mark.parametrize("opt", ["abc", "k2fd", "consistent", "tanh_identity", "no_lin"])
+@pytest.mark.parametrize("n", [64, 128])
+def test_default_fast_path_vs_exact_reference_formula(n):
+    """The default ACDI evaluation (tanh(psi/2eps) as (2phi-1)/(1+2enum), phi
+    floored at 0 inside the log) against the oracle running the reference's
+    exact formulas (FP64 tanh, min(phi,1) only; multi/main.f90:388-389, 463-465)."""
+    p = _params()
+    exact = _params(tanh_identity=0, phi_floor=0)
+    case = _case(n, True, ndrops=4, rmin=0.4, rmax=0.6) if n == 64 else None
+    ref, got, _, _, _, _ = run_pair(n, 10, True, p, case=case, oracle_p=exact)
+    _check(ref, got, True)
+
+
+@pytest.mark.parametrize("opt", ["abc", "k2fd", "consistent", "exact_tanh", "no_lin"])
 def test_options_32(opt):
     kw = {"abc": dict(f1=0.3, f2=0.2, f3=0.1, k0=2.0), "k2fd": dict(k2_mode=1),
-          "consistent": dict(grid_mode=1), "tanh_identity": dict(tanh_identity=1),
+          "consistent": dict(grid_mode=1), "exact_tanh": dict(tanh_identity=0, phi_floor=0),
           "no_lin": dict(lin_force=0.0)}[opt]
     p = _params(**kw)
     case = _case(32, True, ndrops=2, rmin=0.6, rmax=0.8, grid_mode=p.grid_mode)
