@@ -37,6 +37,7 @@ extern "C" {
 #define MHIT_ERR_IO 6          /* field file missing or of the wrong size */
 #define MHIT_ERR_UNSUPPORTED 7 /* grid size or option not built */
 #define MHIT_ERR_STATE 8       /* call out of order (e.g. step before set_fields) */
+#define MHIT_ERR_SCRATCH_LIMIT 9 /* grid larger than the fixed scratch of mhit_poisson_noalloc */
 
 /* Field layouts for set/get. */
 #define MHIT_LAYOUT_RAW 0      /* (nx, ny, nz), the .dat interior (multi/readwrite.f90:29) */
@@ -217,6 +218,24 @@ int mhit_step_async(mhit_handle* h, int nsteps);
 void* mhit_stream(mhit_handle* h);
 const char* mhit_last_error(mhit_handle* h);
 
+/*
+ * Allocation-free Poisson solve (no counterpart in the reference).  For
+ * callers that cannot let a library allocate device memory -- an application
+ * whose device memory is all owned by its own allocator, or a latency-critical
+ * loop that cannot absorb the device-wide synchronisation of cudaFree.  Solves
+ * the same problem as mhit_poisson_device (rhs_dev -> p_dev, n^3 float64 on
+ * the device, raw layout, k2_mode / grid_mode as in mhit_params) on `stream`
+ * (a cudaStream_t, NULL for the default stream), without a handle and without
+ * cudaMalloc/cudaFree: its scratch (half spectrum and tables) is a fixed
+ * device array of the library for n <= MHIT_NOALLOC_MAX_N (18.9 MB, held on
+ * every GPU that loads the library until exit).  Larger n returns
+ * MHIT_ERR_SCRATCH_LIMIT.  The first call on a device resolves the scratch
+ * address, so make it before any stream capture.  All calls share the
+ * scratch: calls that overlap on the GPU race and must be serialised.
+ */
+#define MHIT_NOALLOC_MAX_N 128
+int mhit_poisson_noalloc(const double* rhs_dev, double* p_dev, int n, int k2_mode, int grid_mode,
+                         void* stream);
 
 /* Free everything (multi/main.f90:979-985). */
 int mhit_destroy(mhit_handle* h);

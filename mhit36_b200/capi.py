@@ -20,6 +20,8 @@ MHIT_ERR_NONFINITE = 5
 MHIT_ERR_IO = 6
 MHIT_ERR_UNSUPPORTED = 7
 MHIT_ERR_STATE = 8
+MHIT_ERR_SCRATCH_LIMIT = 9
+MHIT_NOALLOC_MAX_N = 128
 
 MHIT_LAYOUT_RAW = 0
 MHIT_LAYOUT_PIX_HALO = 1
@@ -71,7 +73,7 @@ HEADER_SYMBOLS = [
     "mhit_step", "mhit_get_diag", "mhit_save", "mhit_load", "mhit_poisson", "mhit_poisson_device",
     "mhit_device_state", "mhit_sync_state", "mhit_memory_bytes", "mhit_launches_per_step",
     "mhit_destroy", "mhit_strerror", "mhit_size_supported", "mhit_profile_step", "mhit_stage_name",
-    "mhit_step_async", "mhit_stream", "mhit_last_error", "mhit_diagnostics",
+    "mhit_step_async", "mhit_stream", "mhit_last_error", "mhit_diagnostics", "mhit_poisson_noalloc",
 ]
 
 _lib = None
@@ -115,6 +117,7 @@ def load_library(path: str = LIB_PATH):
         "mhit_profile_step": (ctypes.c_int, [H, ctypes.c_int, P(ctypes.c_double), P(ctypes.c_int)]),
         "mhit_stage_name": (ctypes.c_char_p, [H, ctypes.c_int]),
         "mhit_diagnostics": (ctypes.c_int, [H, ctypes.c_int, P(MhitStats)]),
+        "mhit_poisson_noalloc": (ctypes.c_int, [dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -399,6 +399,7 @@ const char* mhit_strerror(int s) {
     case MHIT_ERR_IO: return "field file missing or of the wrong size";
     case MHIT_ERR_UNSUPPORTED: return "unsupported grid size or option";
     case MHIT_ERR_STATE: return "call out of order";
+    case MHIT_ERR_SCRATCH_LIMIT: return "grid larger than the fixed scratch of the allocation-free entry point";
     default: return "unknown status";
   }
 }

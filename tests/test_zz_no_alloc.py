@@ -1,0 +1,52 @@
+"""GPU test of mhit_poisson_noalloc, the Poisson solve for callers that cannot
+let the library allocate device memory (their device memory belongs to their
+own allocator, or they cannot absorb cudaFree's device-wide synchronisation).
+
+It is called through the C ABI and checked against the handle-based
+mhit_poisson_device on the same device inputs, on two calls in a row (the
+scratch keeps the previous call's contents).  This file sorts last so that a
+run stopping at the first failure has already run every other test.
+"""
+import ctypes
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-13  # the Poisson tolerance of tests/test_gpu_parity.py
+
+
+def _rel(a, b):
+    return float((a - b).abs().max() / b.abs().max())
+
+
+@pytest.mark.parametrize("n,k2_mode,grid_mode", [(64, 0, 0), (128, 1, 1)])
+def test_noalloc_matches_handle_solve_twice(n, k2_mode, grid_mode):
+    import torch
+    from mhit36_b200 import Solver, capi
+    from mhit36_b200.config import InputParams
+    lib = capi.load_library()
+    gen = torch.Generator(device="cuda").manual_seed(n)
+    rhs = [torch.randn(n ** 3, dtype=torch.float64, device="cuda", generator=gen) for _ in range(2)]
+    ref = [torch.empty_like(r) for r in rhs]
+    with Solver(n, InputParams(k2_mode=k2_mode, grid_mode=grid_mode), phase_field=False) as s:
+        for r, o in zip(rhs, ref):
+            s.poisson_device(r.data_ptr(), o.data_ptr())
+        torch.cuda.synchronize()
+    for r, o in zip(rhs, ref):  # two calls in a row share the scratch
+        got = torch.full_like(r, float("nan"))
+        rc = lib.mhit_poisson_noalloc(r.data_ptr(), got.data_ptr(), n, k2_mode, grid_mode, None)
+        assert rc == capi.MHIT_OK, lib.mhit_strerror(rc)
+        torch.cuda.synchronize()
+        assert _rel(got, o) <= TOL
+
+
+def test_noalloc_rejects_sizes_beyond_scratch():
+    import torch
+    from mhit36_b200 import capi
+    lib = capi.load_library()
+    n = 2 * capi.MHIT_NOALLOC_MAX_N
+    rhs = torch.zeros(8, dtype=torch.float64, device="cuda")
+    rc = lib.mhit_poisson_noalloc(rhs.data_ptr(), rhs.data_ptr(), n, 0, 0, None)
+    assert rc == capi.MHIT_ERR_SCRATCH_LIMIT
+    assert b"scratch" in lib.mhit_strerror(rc)
