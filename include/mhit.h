@@ -154,6 +154,17 @@ int mhit_step(mhit_handle* h, int nsteps, mhit_diag* out);
  */
 int mhit_diagnostics(mhit_handle* h, int pi_f32, mhit_stats* out);
 
+/*
+ * Drop count and size distribution of the current phi, as the reference's
+ * post-processor post/DropCountSize computes it: cells with phi >= 0.5
+ * (get_interface.f90:15), 26-connected with periodic wrap (flood_fill.f90),
+ * numbered in the order the x-fastest scan meets each drop's first cell
+ * (get_interface.f90:28-47).  *ndrops = number of drops; for the first
+ * `capacity` of them cells[i] = cell count and deq[i] = dx*(6*cells/pi)^(1/3)
+ * (calculate_deq.f90:29-33), dx the handle's grid spacing.
+ */
+int mhit_drop_count(mhit_handle* h, int capacity, int* ndrops, int64_t* cells, double* deq);
+
 /* Read the current per-step scalars without stepping. */
 int mhit_get_diag(mhit_handle* h, mhit_diag* out);
 
@@ -193,6 +204,11 @@ int mhit_device_state(mhit_handle* h, void** u, void** v, void** w, void** phi);
 
 /* Apply the pending mean removal to the resident u, v, w in place. */
 int mhit_sync_state(mhit_handle* h);
+
+/* Tile shapes of the stencil kernels: z chunk kz (a divisor of n; 0 = 32)
+ * and momentum tile height mty (8 or 16; 0 = the default for n).  Results do
+ * not depend on them; the step graphs are re-captured on the next step. */
+int mhit_set_tiles(mhit_handle* h, int kz, int mty);
 
 /* Bytes of device memory the handle holds. */
 int mhit_memory_bytes(mhit_handle* h, size_t* bytes);
@@ -236,6 +252,58 @@ const char* mhit_last_error(mhit_handle* h);
 #define MHIT_NOALLOC_MAX_N 128
 int mhit_poisson_noalloc(const double* rhs_dev, double* p_dev, int n, int k2_mode, int grid_mode,
                          void* stream);
+
+/* ------------------------------------------------------------------------
+ * Served ensemble (no counterpart in the reference, which runs one
+ * simulation per job).  Independent simulations of uneven grid sizes are
+ * queued, admitted as slots and HBM free up (the budget is an HBM-footprint
+ * admission limit), kept resident, and advanced together: the simulations of
+ * one class (n, precision, phase field, k2_mode, grid_mode) share one CUDA
+ * graph of batched kernels that read per-slot arguments from a device table,
+ * so admission never re-captures.  Classes run on their own streams.  Each
+ * slot computes exactly what mhit_step computes for the same request.
+ * ---------------------------------------------------------------------- */
+typedef struct mhit_ensemble mhit_ensemble;
+
+#define MHIT_RQ_QUEUED 0
+#define MHIT_RQ_RUNNING 1
+#define MHIT_RQ_DONE 2
+#define MHIT_RQ_FAILED 3
+#define MHIT_RQ_CANCELLED 4
+
+typedef struct mhit_ens_info {
+  int32_t state;        /* MHIT_RQ_* */
+  int32_t status;       /* MHIT_OK or the request's error */
+  int32_t n;
+  int32_t steps_issued; /* steps enqueued so far */
+  double t_submit, t_admit, t_done; /* seconds since mhit_ens_create (-1: not yet) */
+  mhit_diag diag;       /* final per-step scalars (done or failed) */
+  int32_t kz;           /* the autotuned tile shape of the request's class: stencil z chunk */
+  int32_t mty;          /* and momentum tile height */
+} mhit_ens_info;
+
+typedef struct mhit_ens_stats_t {
+  int64_t rounds, graph_launches;
+  size_t bytes_used, bytes_budget;
+  int32_t classes, slots;
+} mhit_ens_stats_t;
+
+/* hbm_budget_bytes = 0: 85% of the free device memory. */
+int mhit_ens_create(size_t hbm_budget_bytes, int slots_per_class, mhit_ensemble** out);
+/* Queue a request (inputs are copied; raw layout float64). */
+int mhit_ens_submit(mhit_ensemble* e, const mhit_params* p, int n, int precision, int phase_field, int nsteps,
+                    const double* u, const double* v, const double* w, const double* phi, int keep_result,
+                    int64_t* id);
+/* One scheduling round: complete, admit, advance every busy class one step. */
+int mhit_ens_progress(mhit_ensemble* e, int* pending);
+int mhit_ens_query(mhit_ensemble* e, int64_t id, mhit_ens_info* out);
+/* Final fields of a done request (keep_result = 1), raw layout float64. */
+int mhit_ens_result(mhit_ensemble* e, int64_t id, double* u, double* v, double* w, double* phi);
+int mhit_ens_release(mhit_ensemble* e, int64_t id);
+int mhit_ens_cancel(mhit_ensemble* e, int64_t id);
+int mhit_ens_stats(mhit_ensemble* e, mhit_ens_stats_t* out);
+const char* mhit_ens_last_error(mhit_ensemble* e);
+int mhit_ens_destroy(mhit_ensemble* e);
 
 /* Free everything (multi/main.f90:979-985). */
 int mhit_destroy(mhit_handle* h);

@@ -67,6 +67,19 @@ class MhitStats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
 
 
+class MhitEnsInfo(ctypes.Structure):
+    _fields_ = [("state", ctypes.c_int32), ("status", ctypes.c_int32), ("n", ctypes.c_int32),
+                ("steps_issued", ctypes.c_int32), ("t_submit", ctypes.c_double), ("t_admit", ctypes.c_double),
+                ("t_done", ctypes.c_double), ("diag", MhitDiag), ("kz", ctypes.c_int32), ("mty", ctypes.c_int32)]
+
+
+class MhitEnsStats(ctypes.Structure):
+    _fields_ = [("rounds", ctypes.c_int64), ("graph_launches", ctypes.c_int64), ("bytes_used", ctypes.c_size_t),
+                ("bytes_budget", ctypes.c_size_t), ("classes", ctypes.c_int32), ("slots", ctypes.c_int32)]
+
+
+RQ_QUEUED, RQ_RUNNING, RQ_DONE, RQ_FAILED, RQ_CANCELLED = range(5)
+
 # Every symbol include/mhit.h declares (checked by the CPU tests).
 HEADER_SYMBOLS = [
     "mhit_default_params", "mhit_create", "mhit_set_fields", "mhit_get_fields", "mhit_get_pressure",
@@ -74,6 +87,9 @@ HEADER_SYMBOLS = [
     "mhit_device_state", "mhit_sync_state", "mhit_memory_bytes", "mhit_launches_per_step",
     "mhit_destroy", "mhit_strerror", "mhit_size_supported", "mhit_profile_step", "mhit_stage_name",
     "mhit_step_async", "mhit_stream", "mhit_last_error", "mhit_diagnostics", "mhit_poisson_noalloc",
+    "mhit_ens_create", "mhit_ens_submit", "mhit_ens_progress", "mhit_ens_query", "mhit_ens_result",
+    "mhit_ens_release", "mhit_ens_cancel", "mhit_ens_stats", "mhit_ens_last_error", "mhit_ens_destroy",
+    "mhit_set_tiles", "mhit_drop_count",
 ]
 
 _lib = None
@@ -118,6 +134,19 @@ def load_library(path: str = LIB_PATH):
         "mhit_stage_name": (ctypes.c_char_p, [H, ctypes.c_int]),
         "mhit_diagnostics": (ctypes.c_int, [H, ctypes.c_int, P(MhitStats)]),
         "mhit_poisson_noalloc": (ctypes.c_int, [dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
+        "mhit_ens_create": (ctypes.c_int, [ctypes.c_size_t, ctypes.c_int, P(H)]),
+        "mhit_ens_submit": (ctypes.c_int, [H, P(MhitParams), ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                           dp, dp, dp, dp, ctypes.c_int, P(ctypes.c_int64)]),
+        "mhit_ens_progress": (ctypes.c_int, [H, P(ctypes.c_int)]),
+        "mhit_ens_query": (ctypes.c_int, [H, ctypes.c_int64, P(MhitEnsInfo)]),
+        "mhit_ens_result": (ctypes.c_int, [H, ctypes.c_int64, dp, dp, dp, dp]),
+        "mhit_ens_release": (ctypes.c_int, [H, ctypes.c_int64]),
+        "mhit_ens_cancel": (ctypes.c_int, [H, ctypes.c_int64]),
+        "mhit_ens_stats": (ctypes.c_int, [H, P(MhitEnsStats)]),
+        "mhit_ens_last_error": (ctypes.c_char_p, [H]),
+        "mhit_ens_destroy": (ctypes.c_int, [H]),
+        "mhit_set_tiles": (ctypes.c_int, [H, ctypes.c_int, ctypes.c_int]),
+        "mhit_drop_count": (ctypes.c_int, [H, ctypes.c_int, P(ctypes.c_int), dp, dp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

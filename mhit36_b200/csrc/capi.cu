@@ -11,6 +11,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <algorithm>
 #include <functional>
 #include <string>
 #include <vector>
@@ -55,6 +56,14 @@ struct mhit_handle {
   Ctrl* h_ctrl = nullptr;  // pinned mirror
   long long nstep_host = 0;
   bool has_fields = false;
+  // drop counting scratch (allocated on first use)
+  int* ccl_lab = nullptr;
+  int* ccl_cnt = nullptr;
+  int2* ccl_roots = nullptr;
+  int* ccl_counter = nullptr;
+  int ccl_cap = 0;
+  int kz = 0;   // stencil z chunk (0: default)
+  int mty = 0;  // momentum tile height (0: default for the grid size)
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   size_t bytes = 0;
   std::vector<void*> allocs;
@@ -164,6 +173,7 @@ std::vector<Stage> step_stages(mhit_handle* h, int cur) {
   std::vector<Stage> v;
   cudaStream_t st = h->st;
   const int n = h->n;
+  const int kz = h->kz, mty = h->mty ? h->mty : mhit::default_mty(n);
   const bool pf = h->phase_field != 0;
   static const char* pnames[5] = {"xfwd", "yfwd", "zsolve", "yinv", "xinv"};
   static const char* rnames[5] = {"xres", "yfwd2", "zsolve2", "yinv2", "xinv2"};
@@ -171,10 +181,10 @@ std::vector<Stage> step_stages(mhit_handle* h, int cur) {
     mhit::StencilArgs<double> a = stencil_args<double>(h, cur);
     mhit::StencilArgs<double> am = a;
     if (pf) {
-      v.push_back({"phase", [a, st] { return mhit::launch_phase<double>(a, st); }});
+      v.push_back({"phase", [a, st, kz] { return mhit::launch_phase<double>(a, st, kz); }});
       am.phi_in = h->phi[cur ^ 1];  // momentum reads the updated phi
     }
-    v.push_back({"momentum", [am, pf, st] { return mhit::launch_momentum<double>(am, pf, st); }});
+    v.push_back({"momentum", [am, pf, st, kz, mty] { return mhit::launch_momentum<double>(am, pf, st, kz, mty); }});
     mhit::PoissonArgs<double> pa;
     pa.us = h->us; pa.vs = h->vs; pa.ws = h->ws;
     pa.spec = h->spec; pa.p = h->p; pa.tw = h->tw; pa.k2tab = h->k2tab; pa.ctrl = h->ctrl;
@@ -191,10 +201,10 @@ std::vector<Stage> step_stages(mhit_handle* h, int cur) {
     mhit::StencilArgs<float> a = stencil_args<float>(h, cur);
     mhit::StencilArgs<float> am = a;
     if (pf) {
-      v.push_back({"phase", [a, st] { return mhit::launch_phase<float>(a, st); }});
+      v.push_back({"phase", [a, st, kz] { return mhit::launch_phase<float>(a, st, kz); }});
       am.phi_in = h->fphi[cur ^ 1];
     }
-    v.push_back({"momentum", [am, pf, st] { return mhit::launch_momentum<float>(am, pf, st); }});
+    v.push_back({"momentum", [am, pf, st, kz, mty] { return mhit::launch_momentum<float>(am, pf, st, kz, mty); }});
     mhit::PoissonArgs<float> pa;
     pa.us = h->fus; pa.vs = h->fvs; pa.ws = h->fws;
     pa.spec = h->fspec; pa.p = h->fp0; pa.tw = h->ftw; pa.k2tab = h->k2tab; pa.ctrl = h->ctrl;
@@ -733,6 +743,68 @@ int mhit_device_state(mhit_handle* h, void** u, void** v, void** w, void** phi) 
     CK(h, pull_ctrl(h));
     *phi = h->phase_field ? fphi(h, (int)(h->h_ctrl->nstep & 1)).ptr : nullptr;
   }
+  return MHIT_OK;
+}
+
+// Drop count and sizes of the current phi (post/DropCountSize): components of
+// phi >= 0.5, 26-connected with periodic wrap, in the reference's scan order.
+int mhit_drop_count(mhit_handle* h, int capacity, int* ndrops, int64_t* cells, double* deq) {
+  if (!h || !ndrops || capacity < 0 || (capacity > 0 && (!cells || !deq))) return MHIT_ERR_INVALID;
+  if (!h->phase_field) return MHIT_ERR_STATE;
+  if (!h->has_fields) return MHIT_ERR_STATE;
+  DeviceGuard g(h->device);
+  const int n = h->n;
+  const size_t N3 = (size_t)n * n * n;
+  if (!h->ccl_lab) {
+    h->ccl_cap = 1 << 20;
+    CK(h, dalloc(h, &h->ccl_lab, N3 * sizeof(int)));
+    CK(h, dalloc(h, &h->ccl_cnt, N3 * sizeof(int)));
+    CK(h, dalloc(h, &h->ccl_roots, (size_t)h->ccl_cap * sizeof(int2)));
+    CK(h, dalloc(h, &h->ccl_counter, 2 * sizeof(int)));
+  }
+  CK(h, pull_ctrl(h));
+  const int cur = (int)(h->h_ctrl->nstep & 1);
+  if (f32(h))
+    CK(h, mhit::launch_dropcount<float>(h->fphi[cur], n, h->ccl_lab, h->ccl_cnt, h->ccl_roots, h->ccl_cap,
+                                        h->ccl_counter, h->st));
+  else
+    CK(h, mhit::launch_dropcount<double>(h->phi[cur], n, h->ccl_lab, h->ccl_cnt, h->ccl_roots, h->ccl_cap,
+                                         h->ccl_counter, h->st));
+  int cnt[2] = {0, 0};
+  CK(h, cudaMemcpyAsync(cnt, h->ccl_counter, sizeof(cnt), cudaMemcpyDeviceToHost, h->st));
+  CK(h, cudaStreamSynchronize(h->st));
+  if (cnt[1]) return MHIT_ERR_CUDA;
+  if (cnt[0] > h->ccl_cap) return MHIT_ERR_UNSUPPORTED;  // more components than the root list holds
+  std::vector<int2> roots(cnt[0]);
+  if (cnt[0] > 0)
+    CK(h, cudaMemcpy(roots.data(), h->ccl_roots, cnt[0] * sizeof(int2), cudaMemcpyDeviceToHost));
+  std::sort(roots.begin(), roots.end(), [](const int2& a, const int2& b) { return a.x < b.x; });
+  const double pi = 4.0 * atan(1.0), n6opi = 6.0 / pi;  // post/DropCountSize/module.f90:3-5
+  const double dx = 1.0 / h->c.dxi;
+  for (int q = 0; q < cnt[0] && q < capacity; ++q) {
+    cells[q] = roots[q].y;
+    deq[q] = dx * pow(n6opi * (double)roots[q].y, 1.0 / 3.0);  // calculate_deq.f90:33
+  }
+  *ndrops = cnt[0];
+  return MHIT_OK;
+}
+
+// Tile shapes of the stencil kernels: z chunk kz (a divisor of n, 0 =
+// default 32) and momentum tile height mty (8 or 16, 0 = default for n).
+// Results do not depend on them; the step graphs are re-captured.
+int mhit_set_tiles(mhit_handle* h, int kz, int mty) {
+  if (!h) return MHIT_ERR_INVALID;
+  if (kz != 0 && !mhit::stencil_kz_ok(h->n, kz)) return MHIT_ERR_INVALID;
+  if (mty != 0 && mty != 8 && mty != 16) return MHIT_ERR_INVALID;
+  DeviceGuard g(h->device);
+  CK(h, cudaStreamSynchronize(h->st));
+  for (int i = 0; i < 2; ++i)
+    if (h->graph[i]) {
+      cudaGraphExecDestroy(h->graph[i]);
+      h->graph[i] = nullptr;
+    }
+  h->kz = kz;
+  h->mty = mty;
   return MHIT_OK;
 }
 

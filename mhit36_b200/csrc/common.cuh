@@ -43,9 +43,12 @@ __device__ __forceinline__ size_t gidx(int i, int j, int k, int n) {
 // One element per call (4 or 8 bytes); a thread's copies land in issue
 // order groups: commit after a batch, wait until at most N groups are pending.
 template <class T> __device__ __forceinline__ void cp_async_elem(T* smem_dst, const T* gmem_src) {
-  static_assert(sizeof(T) == 4 || sizeof(T) == 8, "cp.async element size");
+  static_assert(sizeof(T) == 4 || sizeof(T) == 8 || sizeof(T) == 16, "cp.async element size");
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gmem_src), "n"(sizeof(T)) : "memory");
+  if constexpr (sizeof(T) == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem_src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gmem_src), "n"(sizeof(T)) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N> __device__ __forceinline__ void cp_async_wait() {

@@ -1,0 +1,839 @@
+// Served ensemble: many independent MHIT36 simulations on one GPU.
+//
+// Requests (grid size, parameters, initial fields, step count) are queued
+// and admitted as slots and HBM free up (continuous batching).  Simulations
+// of the same class -- grid size, precision form, phase field, k^2 and grid
+// conventions -- advance together: one CUDA graph per class holds the
+// batched kernels of one step for all of the class's slots, and each kernel
+// reads its per-slot arguments from a device slot table, so admitting or
+// retiring a request only rewrites that table (no re-capture).  Classes run on
+// their own streams, so their work overlaps on the device.  Each slot runs
+// exactly the arithmetic of a single simulation (own control block, own
+// deterministic reductions), so a result does not depend on the mix.
+//
+// The stencil kernels' z chunk of a class comes from an online autotuner:
+// the first rounds of a class time the candidates on live data with CUDA
+// events, then the class graph is re-captured once with the fastest.
+//
+// There is no counterpart in the reference, which runs one simulation per job.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <chrono>
+#include <deque>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+#include "mhit.h"
+
+using mhit::Ctrl;
+using mhit::SlotArgs;
+using mhit::StepConst;
+
+namespace {
+
+double now_s() {
+  using namespace std::chrono;
+  return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+enum { RQ_QUEUED = 0, RQ_RUNNING = 1, RQ_DONE = 2, RQ_FAILED = 3, RQ_CANCELLED = 4 };
+
+struct Request {
+  int64_t id = 0;
+  int n = 0, pf = 0, precision = 0, nsteps = 0, keep = 1;
+  mhit_params prm;
+  std::vector<double> in[4];   // initial u, v, w, phi (raw layout), dropped at admission
+  std::vector<double> out[4];  // final fields when keep = 1
+  int state = RQ_QUEUED;
+  int cls = -1, slot = -1;
+  int steps_issued = 0;
+  int status = MHIT_OK;
+  double t_submit = 0, t_admit = 0, t_done = 0;
+  mhit_diag diag;
+  cudaEvent_t done_ev = nullptr;  // recorded after the request's last step
+  bool finishing = false;
+  void* pinned = nullptr;  // D2H staging of the final fields and control block
+};
+
+// Device buffers of one slot (either precision; unused pointers stay null).
+struct SlotBuf {
+  bool allocated = false;
+  size_t bytes = 0;
+  std::vector<void*> ptrs;
+  void* f[16] = {nullptr};  // u v w us vs ws ru rv rw phi0 phi1 p/p0 dp spec partials fsin|fcos
+  double* fsin = nullptr;
+  double* fcos = nullptr;
+  Ctrl* ctrl = nullptr;      // into the class's contiguous ctrl array
+  int64_t req = -1;          // running request, or -1
+};
+
+struct Class {
+  int n = 0, pf = 0, precision = 0, k2_mode = 0, grid_mode = 0;
+  int nslots = 0;
+  int kz = 32, mty = 16;
+  cudaStream_t st = nullptr;
+  void* d_slots = nullptr;   // SlotArgs<T>[nslots]
+  Ctrl* d_ctrl = nullptr;    // [nslots]
+  Ctrl* h_ctrl = nullptr;    // pinned mirror
+  void* tw = nullptr;        // twiddles (double2 or float2)
+  double* k2tab = nullptr;
+  std::vector<SlotBuf> slots;
+  std::vector<SlotArgs<double>> hd;  // host copies of the slot tables
+  std::vector<SlotArgs<float>> hf;
+  cudaGraphExec_t graph = nullptr;
+  // autotuner: candidate (kz, mty) tile shapes
+  std::vector<std::pair<int, int>> cand;
+  std::vector<double> cand_ms;
+  std::vector<int> cand_runs;
+  int tune_idx = 0;
+  bool tuned = false;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t inflight[2] = {nullptr, nullptr};  // last two rounds (bounds host run-ahead)
+  int rounds = 0;
+  size_t active() const {
+    size_t a = 0;
+    for (auto& s : slots) a += (s.req >= 0);
+    return a;
+  }
+};
+
+}  // namespace
+
+struct mhit_ensemble {
+  int device = 0;
+  size_t budget = 0, used = 0;
+  int slots_per_class = 8;
+  int64_t next_id = 1;
+  double t0 = 0;
+  std::map<int64_t, std::unique_ptr<Request>> reqs;
+  std::deque<int64_t> queue;
+  std::vector<std::unique_ptr<Class>> classes;
+  std::string last_error;
+  long long rounds = 0, launches = 0;
+};
+
+namespace {
+
+bool built_size(int n) {
+  bool ok = false;
+#define MHIT_CASE(NN) ok |= (n == NN);
+  MHIT_FOR_SIZES(MHIT_CASE)
+#undef MHIT_CASE
+  return ok && mhit::stencil_size_ok(n);
+}
+
+size_t elem(int precision) { return precision == MHIT_FP64 ? sizeof(double) : sizeof(float); }
+
+// Device bytes of one slot of a class.
+size_t slot_bytes(int n, int pf, int precision) {
+  const size_t N3 = (size_t)n * n * n, e = elem(precision);
+  size_t fields = 9 + 1 + (pf ? 2 : 0) + (precision == MHIT_FP64 ? 0 : 1);  // + p / (p0, dp)
+  const size_t spec = (size_t)n * n * mhit::spectrum_pitch(n) * 2 * e;
+  return fields * N3 * e + spec + (size_t)mhit::project_partials(n) * 7 * sizeof(double) + 2 * n * sizeof(double);
+}
+
+StepConst make_const(const mhit_params* p, int n) {
+  StepConst c;
+  memset(&c, 0, sizeof(c));
+  const double twopi = 8.0 * atan(1.0);
+  const double dx = (p->grid_mode == MHIT_GRID_CONSISTENT) ? twopi / n : twopi / (n - 1);
+  c.n = n;
+  c.dt = p->dt; c.mu = p->mu; c.rho = p->rho;
+  c.rhoi = 1.0 / p->rho;
+  c.dxi = 1.0 / dx;
+  c.ddxi = 1.0 / dx / dx;
+  c.eps = p->epsr * dx;
+  c.epsi = 1.0 / c.eps;
+  c.enumv = (double)(float)1.e-16;
+  c.tiny = (double)(float)1.0E-16;
+  c.sigma = p->sigma;
+  c.lin_force = p->lin_force;
+  c.f1 = p->f1; c.f2 = p->f2; c.f3 = p->f3;
+  c.abc = (p->f1 != 0.0 || p->f2 != 0.0 || p->f3 != 0.0) ? 1 : 0;
+  c.tanh_identity = p->tanh_identity ? 1 : 0;
+  c.phi_floor = p->phi_floor ? 1 : 0;
+  c.cdiv = p->rho * c.dxi / p->dt;
+  c.dtr = p->dt / p->rho;
+  return c;
+}
+
+int fail(mhit_ensemble* e, cudaError_t err, const char* where) {
+  e->last_error = std::string(where) + ": " + cudaGetErrorString(err);
+  return err == cudaErrorMemoryAllocation ? MHIT_ERR_NOMEM : MHIT_ERR_CUDA;
+}
+
+#define ECK(e, call)                                        \
+  do {                                                      \
+    cudaError_t e_ = (call);                                \
+    if (e_ != cudaSuccess) return fail(e, e_, #call);       \
+  } while (0)
+
+// Enqueue one batched step of every slot of class c (inactive slots return at once).
+cudaError_t enqueue_class_step(Class* c, int kz, int mty) {
+  const int n = c->n, S = c->nslots;
+  cudaError_t err;
+  if (c->precision == MHIT_FP64) {
+    const SlotArgs<double>* t = static_cast<const SlotArgs<double>*>(c->d_slots);
+    if (c->pf && (err = mhit::launch_phase_batched<double>(t, S, n, kz, c->st))) return err;
+    if ((err = mhit::launch_momentum_batched<double>(t, S, n, kz, c->pf != 0, c->st, mty))) return err;
+    for (int k = 0; k < 5; ++k)
+      if ((err = mhit::launch_poisson_stage_batched<double>(t, S, n, k, 0, c->st))) return err;
+    if ((err = mhit::launch_project_batched<double>(t, S, n, c->st))) return err;
+    return mhit::launch_finalize_batched(t, S, n, c->st);
+  }
+  const SlotArgs<float>* t = static_cast<const SlotArgs<float>*>(c->d_slots);
+  if (c->pf && (err = mhit::launch_phase_batched<float>(t, S, n, kz, c->st))) return err;
+  if ((err = mhit::launch_momentum_batched<float>(t, S, n, kz, c->pf != 0, c->st, mty))) return err;
+  for (int w = 0; w < 2; ++w)
+    for (int k = 0; k < 5; ++k)
+      if ((err = mhit::launch_poisson_stage_batched<float>(t, S, n, k, w, c->st))) return err;
+  if ((err = mhit::launch_project_batched<float>(t, S, n, c->st))) return err;
+  return mhit::launch_finalize_batched_f32(t, S, n, c->st);
+}
+
+cudaError_t capture_class(Class* c, int kz, int mty) {
+  if (c->graph) {
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+  }
+  cudaGraph_t g = nullptr;
+  cudaError_t err = cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal);
+  if (err) return err;
+  cudaError_t e2 = enqueue_class_step(c, kz, mty);
+  err = cudaStreamEndCapture(c->st, &g);
+  if (e2) {
+    if (g) cudaGraphDestroy(g);
+    return e2;
+  }
+  if (err) return err;
+  err = cudaGraphInstantiate(&c->graph, g, 0);
+  cudaGraphDestroy(g);
+  return err;
+}
+
+int class_for(mhit_ensemble* e, const Request* r) {
+  for (size_t i = 0; i < e->classes.size(); ++i) {
+    Class* c = e->classes[i].get();
+    if (c->n == r->n && c->pf == r->pf && c->precision == r->precision && c->k2_mode == r->prm.k2_mode &&
+        c->grid_mode == r->prm.grid_mode)
+      return (int)i;
+  }
+  return -1;
+}
+
+// Create a class (stream, tables, empty slot table, graph).
+int make_class(mhit_ensemble* e, const Request* r, int* out) {
+  std::unique_ptr<Class> c(new Class());
+  c->n = r->n; c->pf = r->pf; c->precision = r->precision;
+  c->k2_mode = r->prm.k2_mode; c->grid_mode = r->prm.grid_mode;
+  const int n = c->n;
+  // slots: as many as the grid dimension limit allows, capped by the setting
+  c->nslots = std::max(1, std::min(e->slots_per_class, 65535 / n));
+  ECK(e, mhit::prepare_stencils());
+  ECK(e, mhit::prepare_poisson(n));
+  ECK(e, cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+  ECK(e, cudaEventCreate(&c->ev0));
+  ECK(e, cudaEventCreate(&c->ev1));
+  const size_t tsz = (c->precision == MHIT_FP64) ? sizeof(SlotArgs<double>) : sizeof(SlotArgs<float>);
+  ECK(e, cudaMalloc(&c->d_slots, tsz * c->nslots));
+  ECK(e, cudaMalloc(&c->d_ctrl, sizeof(Ctrl) * c->nslots));
+  ECK(e, cudaMallocHost(&c->h_ctrl, sizeof(Ctrl) * c->nslots));
+  memset(c->h_ctrl, 0, sizeof(Ctrl) * c->nslots);
+  // tables (same values as mhit_create builds)
+  const double twopi = 8.0 * atan(1.0), lx = twopi;
+  const double dx = (c->grid_mode == MHIT_GRID_CONSISTENT) ? lx / n : lx / (n - 1);
+  const double ddxi = 1.0 / dx / dx, pi = 4.0 * atan(1.0);
+  std::vector<double> k2(n);
+  std::vector<double2> twd(n);
+  std::vector<float2> twf(n);
+  for (int m = 0; m < n; ++m) {
+    long double a = 2.0L * 3.141592653589793238462643383279502884L * (long double)m / (long double)n;
+    twd[m].x = (double)cosl(a); twd[m].y = -(double)sinl(a);
+    twf[m].x = (float)cosl(a); twf[m].y = -(float)sinl(a);
+    if (c->k2_mode == MHIT_K2_FD) {
+      const double s = sin(pi * m / n);
+      k2[m] = (4.0 * ddxi) * (s * s);
+    } else {
+      const double kk = (m < n / 2 ? (double)m : (double)(m - n)) * (twopi / lx);
+      k2[m] = kk * kk;
+    }
+  }
+  ECK(e, cudaMalloc(&c->k2tab, n * sizeof(double)));
+  ECK(e, cudaMemcpy(c->k2tab, k2.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+  if (c->precision == MHIT_FP64) {
+    ECK(e, cudaMalloc(&c->tw, n * sizeof(double2)));
+    ECK(e, cudaMemcpy(c->tw, twd.data(), n * sizeof(double2), cudaMemcpyHostToDevice));
+    c->hd.assign(c->nslots, SlotArgs<double>());
+    memset((void*)c->hd.data(), 0, sizeof(SlotArgs<double>) * c->nslots);
+    ECK(e, cudaMemcpy(c->d_slots, c->hd.data(), tsz * c->nslots, cudaMemcpyHostToDevice));
+  } else {
+    ECK(e, cudaMalloc(&c->tw, n * sizeof(float2)));
+    ECK(e, cudaMemcpy(c->tw, twf.data(), n * sizeof(float2), cudaMemcpyHostToDevice));
+    c->hf.assign(c->nslots, SlotArgs<float>());
+    memset((void*)c->hf.data(), 0, sizeof(SlotArgs<float>) * c->nslots);
+    ECK(e, cudaMemcpy(c->d_slots, c->hf.data(), tsz * c->nslots, cudaMemcpyHostToDevice));
+  }
+  c->slots.assign(c->nslots, SlotBuf());
+  for (int s = 0; s < c->nslots; ++s) c->slots[s].ctrl = c->d_ctrl + s;
+  // autotuner candidates for the stencil kernels' z chunk
+  for (int kz : {8, 16, 32})
+    for (int mty : {8, 16})
+      if (mhit::stencil_kz_ok(n, kz)) c->cand.push_back(std::make_pair(kz, mty));
+  c->cand_ms.assign(c->cand.size(), 0.0);
+  c->cand_runs.assign(c->cand.size(), 0);
+  c->kz = c->cand.empty() ? 32 : c->cand[0].first;
+  c->mty = c->cand.empty() ? 16 : c->cand[0].second;
+  ECK(e, capture_class(c.get(), c->kz, c->mty));
+  e->classes.push_back(std::move(c));
+  *out = (int)e->classes.size() - 1;
+  return MHIT_OK;
+}
+
+}  // namespace
+
+namespace {
+
+// dst = phi[nstep & 1]: the phi of the slot's last completed step, chosen on
+// the device (a request that stopped early on an error has an odd or even
+// step count the host does not know).
+template <class T>
+__global__ void select_phi_kernel(T* __restrict__ dst, const T* __restrict__ a, const T* __restrict__ b,
+                                  const Ctrl* __restrict__ ctrl, size_t count) {
+  const T* src = (ctrl->nstep & 1) ? b : a;
+  for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < count; g += (size_t)gridDim.x * blockDim.x)
+    dst[g] = src[g];
+}
+
+void free_slot_buffers(mhit_ensemble* e, SlotBuf& b) {
+  for (void* q : b.ptrs) cudaFree(q);
+  b.ptrs.clear();
+  for (auto& f : b.f) f = nullptr;
+  b.fsin = b.fcos = nullptr;
+  e->used -= b.bytes;
+  b.bytes = 0;
+  b.allocated = false;
+}
+
+cudaError_t alloc_slot_buffers(mhit_ensemble* e, Class* c, SlotBuf& b) {
+  const int n = c->n;
+  const size_t N3 = (size_t)n * n * n, el = elem(c->precision);
+  auto get = [&](size_t bytes, void** out) {
+    cudaError_t r = cudaMalloc(out, bytes);
+    if (r == cudaSuccess) {
+      b.ptrs.push_back(*out);
+      b.bytes += bytes;
+      e->used += bytes;
+    }
+    return r;
+  };
+  cudaError_t r;
+  const int nf = 9 + 1 + (c->precision == MHIT_FP64 ? 0 : 1);  // + p (or p0, dp)
+  for (int q = 0; q < 9; ++q)
+    if ((r = get(N3 * el, &b.f[q]))) return r;
+  if (c->pf) {
+    if ((r = get(N3 * el, &b.f[9])) || (r = get(N3 * el, &b.f[10]))) return r;
+  }
+  for (int q = 9; q < nf; ++q)
+    if ((r = get(N3 * el, &b.f[11 + (q - 9)]))) return r;
+  const size_t spec = (size_t)n * n * mhit::spectrum_pitch(n) * 2 * el;
+  if ((r = get(spec, &b.f[13]))) return r;
+  if ((r = cudaMemsetAsync(b.f[13], 0, spec, c->st))) return r;
+  if ((r = get((size_t)mhit::project_partials(n) * 7 * sizeof(double), &b.f[14]))) return r;
+  void* t = nullptr;
+  if ((r = get(2 * n * sizeof(double), &t))) return r;
+  b.fsin = static_cast<double*>(t);
+  b.fcos = b.fsin + n;
+  b.allocated = true;
+  return cudaSuccess;
+}
+
+template <class T> SlotArgs<T> build_args(Class* c, SlotBuf& b, const StepConst& k, int active) {
+  SlotArgs<T> a;
+  memset((void*)&a, 0, sizeof(a));
+  T* f[16];
+  for (int q = 0; q < 16; ++q) f[q] = static_cast<T*>(b.f[q]);
+  a.st.u = f[0]; a.st.v = f[1]; a.st.w = f[2];
+  a.st.us = f[3]; a.st.vs = f[4]; a.st.ws = f[5];
+  a.st.ru = f[6]; a.st.rv = f[7]; a.st.rw = f[8];
+  a.st.p = f[11];
+  a.st.uo = f[0]; a.st.vo = f[1]; a.st.wo = f[2];
+  a.st.partials = static_cast<double*>(b.f[14]);
+  a.st.fsin = b.fsin;
+  a.st.fcos = b.fcos;
+  a.st.ctrl = b.ctrl;
+  a.st.c = k;
+  typedef typename mhit::C2<T>::t CT;
+  a.po.us = f[3]; a.po.vs = f[4]; a.po.ws = f[5];
+  a.po.spec = static_cast<CT*>(b.f[13]);
+  a.po.p = f[11];
+  a.po.tw = static_cast<const CT*>(c->tw);
+  a.po.k2tab = c->k2tab;
+  a.po.ctrl = b.ctrl;
+  a.po.cdiv = k.cdiv;
+  a.po.ddxi = k.ddxi;
+  a.pr = a.po;
+  a.pr.pres = f[11];
+  a.pr.p = f[12];
+  a.phi[0] = f[9];
+  a.phi[1] = f[10];
+  a.dp = static_cast<float*>(b.f[12]);
+  a.active = active;
+  return a;
+}
+
+cudaError_t write_entry(Class* c, int s, const SlotArgs<double>* d, const SlotArgs<float>* f) {
+  if (c->precision == MHIT_FP64) {
+    c->hd[s] = *d;
+    return cudaMemcpyAsync(static_cast<SlotArgs<double>*>(c->d_slots) + s, &c->hd[s], sizeof(SlotArgs<double>),
+                           cudaMemcpyHostToDevice, c->st);
+  }
+  c->hf[s] = *f;
+  return cudaMemcpyAsync(static_cast<SlotArgs<float>*>(c->d_slots) + s, &c->hf[s], sizeof(SlotArgs<float>),
+                         cudaMemcpyHostToDevice, c->st);
+}
+
+cudaError_t set_active(Class* c, int s, int active) {
+  if (c->precision == MHIT_FP64) {
+    SlotArgs<double> a = c->hd[s];
+    a.active = active;
+    return write_entry(c, s, &a, nullptr);
+  }
+  SlotArgs<float> a = c->hf[s];
+  a.active = active;
+  return write_entry(c, s, nullptr, &a);
+}
+
+// host float64 -> slot field (FP32 slots are rounded on the host)
+cudaError_t put(Class* c, void* dst, const std::vector<double>& src) {
+  if (c->precision == MHIT_FP64)
+    return cudaMemcpyAsync(dst, src.data(), src.size() * sizeof(double), cudaMemcpyHostToDevice, c->st);
+  std::vector<float> tmp(src.begin(), src.end());
+  cudaError_t r = cudaMemcpyAsync(dst, tmp.data(), tmp.size() * sizeof(float), cudaMemcpyHostToDevice, c->st);
+  if (r) return r;
+  return cudaStreamSynchronize(c->st);
+}
+
+// Try to start request r; returns 1 when admitted, 0 when it has to wait.
+int admit(mhit_ensemble* e, Request* r, int* err) {
+  *err = MHIT_OK;
+  int ci = class_for(e, r);
+  if (ci < 0) {
+    int rc = make_class(e, r, &ci);
+    if (rc) {
+      *err = rc;
+      return 0;
+    }
+  }
+  Class* c = e->classes[ci].get();
+  int s = -1;
+  for (int q = 0; q < c->nslots && s < 0; ++q)
+    if (c->slots[q].req == -1 && c->slots[q].allocated) s = q;
+  for (int q = 0; q < c->nslots && s < 0; ++q)
+    if (c->slots[q].req == -1) s = q;
+  if (s < 0) return 0;  // class full
+  SlotBuf& b = c->slots[s];
+  if (!b.allocated) {
+    const size_t need = slot_bytes(c->n, c->pf, c->precision);
+    // admission by HBM footprint: reclaim idle pooled slots of other classes
+    for (auto& oc : e->classes) {
+      if (e->used + need <= e->budget) break;
+      if (oc.get() == c) continue;
+      for (auto& ob : oc->slots)
+        if (ob.allocated && ob.req == -1 && e->used + need > e->budget) {
+          cudaStreamSynchronize(oc->st);
+          free_slot_buffers(e, ob);
+        }
+    }
+    if (e->used + need > e->budget) return 0;
+    cudaError_t a = alloc_slot_buffers(e, c, b);
+    if (a) {
+      free_slot_buffers(e, b);
+      cudaGetLastError();
+      return 0;  // device memory tighter than the budget says: wait
+    }
+  }
+  const StepConst k = make_const(&r->prm, c->n);
+  const size_t N3 = (size_t)c->n * c->n * c->n;
+  cudaError_t q;
+#define ACK(call)              \
+  if ((q = (call))) {          \
+    *err = fail(e, q, #call);  \
+    return 0;                  \
+  }
+  ACK(put(c, b.f[0], r->in[0]));
+  ACK(put(c, b.f[1], r->in[1]));
+  ACK(put(c, b.f[2], r->in[2]));
+  if (c->pf) ACK(put(c, b.f[9], r->in[3]));
+  for (int f = 6; f < 9; ++f) ACK(cudaMemsetAsync(b.f[f], 0, N3 * elem(c->precision), c->st));
+  ACK(cudaMemsetAsync(b.f[11], 0, N3 * elem(c->precision), c->st));
+  // ABC forcing tables of this request (multi/main.f90:150-153, 591-593)
+  std::vector<double> tab(2 * c->n), x(c->n);
+  const double twopi = 8.0 * atan(1.0);
+  const double dx = (r->prm.grid_mode == MHIT_GRID_CONSISTENT) ? twopi / c->n : twopi / (c->n - 1);
+  x[0] = 0.0;
+  for (int m = 1; m < c->n; ++m) x[m] = x[m - 1] + dx;
+  for (int m = 0; m < c->n; ++m) {
+    tab[m] = sin(r->prm.k0 * x[m]);
+    tab[c->n + m] = cos(r->prm.k0 * x[m]);
+  }
+  ACK(cudaMemcpyAsync(b.fsin, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
+  Ctrl ctl;
+  memset(&ctl, 0, sizeof(ctl));
+  ctl.gumax = 1.0;  // multi/main.f90:323-325
+  ctl.alpha = 1.0;
+  ctl.beta = 0.0;
+  ctl.cfl_limit = r->prm.cfl_limit > 0 ? r->prm.cfl_limit : 7.0;
+  ACK(cudaMemcpyAsync(b.ctrl, &ctl, sizeof(Ctrl), cudaMemcpyHostToDevice, c->st));
+  if (c->precision == MHIT_FP64) {
+    SlotArgs<double> a = build_args<double>(c, b, k, 1);
+    ACK(write_entry(c, s, &a, nullptr));
+  } else {
+    ACK(cudaMemsetAsync(b.f[12], 0, N3 * sizeof(float), c->st));
+    SlotArgs<float> a = build_args<float>(c, b, k, 1);
+    ACK(write_entry(c, s, nullptr, &a));
+  }
+  ACK(cudaStreamSynchronize(c->st));  // the staged host data may go now
+#undef ACK
+  b.req = r->id;
+  r->cls = ci;
+  r->slot = s;
+  r->state = RQ_RUNNING;
+  r->t_admit = now_s();
+  for (auto& v : r->in) std::vector<double>().swap(v);
+  return 1;
+}
+
+// After the request's last step: materialise the mean removal, stage the
+// fields and the control block for the host, record the completion event and
+// take the slot out of the batch -- all in stream order.
+cudaError_t retire_enqueue(mhit_ensemble* e, Class* c, Request* r) {
+  SlotBuf& b = c->slots[r->slot];
+  const size_t N3 = (size_t)c->n * c->n * c->n, el = elem(c->precision);
+  cudaError_t q;
+  if (c->precision == MHIT_FP64)
+    q = mhit::launch_materialize<double>(static_cast<double*>(b.f[0]), static_cast<double*>(b.f[1]),
+                                         static_cast<double*>(b.f[2]), c->n, b.ctrl, c->st);
+  else
+    q = mhit::launch_materialize<float>(static_cast<float*>(b.f[0]), static_cast<float*>(b.f[1]),
+                                        static_cast<float*>(b.f[2]), c->n, b.ctrl, c->st);
+  if (q) return q;
+  const size_t nf = r->keep ? (c->pf ? 4 : 3) : 0;
+  if ((q = cudaMallocHost(&r->pinned, nf * N3 * el + sizeof(Ctrl)))) return q;
+  char* hp = static_cast<char*>(r->pinned);
+  if ((q = cudaMemcpyAsync(hp, b.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, c->st))) return q;
+  hp += sizeof(Ctrl);
+  // phi of the last completed step, staged through the (now idle) spectrum buffer
+  if (c->pf && r->keep) {
+    if (c->precision == MHIT_FP64)
+      select_phi_kernel<double><<<1184, 256, 0, c->st>>>(static_cast<double*>(b.f[13]), static_cast<double*>(b.f[9]),
+                                                        static_cast<double*>(b.f[10]), b.ctrl, N3);
+    else
+      select_phi_kernel<float><<<1184, 256, 0, c->st>>>(static_cast<float*>(b.f[13]), static_cast<float*>(b.f[9]),
+                                                       static_cast<float*>(b.f[10]), b.ctrl, N3);
+    if ((q = cudaGetLastError())) return q;
+  }
+  void* src[4] = {b.f[0], b.f[1], b.f[2], b.f[13]};
+  for (size_t f = 0; f < nf; ++f)
+    if ((q = cudaMemcpyAsync(hp + f * N3 * el, src[f], N3 * el, cudaMemcpyDeviceToHost, c->st))) return q;
+  if ((q = cudaEventCreateWithFlags(&r->done_ev, cudaEventDisableTiming))) return q;
+  if ((q = cudaEventRecord(r->done_ev, c->st))) return q;
+  if ((q = set_active(c, r->slot, 0))) return q;
+  b.req = -2;  // retiring: buffers busy until done_ev
+  r->finishing = true;
+  (void)e;
+  return cudaSuccess;
+}
+
+void complete(mhit_ensemble* e, Request* r) {
+  Class* c = e->classes[r->cls].get();
+  const size_t N3 = (size_t)c->n * c->n * c->n, el = elem(c->precision);
+  const char* hp = static_cast<const char*>(r->pinned);
+  Ctrl ctl;
+  memcpy(&ctl, hp, sizeof(Ctrl));
+  hp += sizeof(Ctrl);
+  const size_t nf = r->keep ? (c->pf ? 4 : 3) : 0;
+  for (size_t f = 0; f < nf; ++f) {
+    r->out[f].resize(N3);
+    if (el == sizeof(double)) {
+      memcpy(r->out[f].data(), hp + f * N3 * el, N3 * el);
+    } else {
+      const float* fp = reinterpret_cast<const float*>(hp + f * N3 * el);
+      for (size_t q = 0; q < N3; ++q) r->out[f][q] = (double)fp[q];
+    }
+  }
+  cudaFreeHost(r->pinned);
+  r->pinned = nullptr;
+  cudaEventDestroy(r->done_ev);
+  r->done_ev = nullptr;
+  r->diag.umax = ctl.gumax;
+  r->diag.cfl = ctl.cfl;
+  r->diag.umean = ctl.last_mean[0];
+  r->diag.vmean = ctl.last_mean[1];
+  r->diag.wmean = ctl.last_mean[2];
+  r->diag.gamma = ctl.gumax;
+  r->diag.max_div = ctl.max_div;
+  r->diag.step = ctl.nstep;
+  r->diag.status = ctl.status;
+  r->status = ctl.status;
+  r->state = ctl.status ? RQ_FAILED : RQ_DONE;
+  r->t_done = now_s();
+  r->finishing = false;
+  c->slots[r->slot].req = -1;  // slot free, buffers pooled
+}
+
+}  // namespace
+
+extern "C" {
+
+int mhit_ens_create(size_t hbm_budget_bytes, int slots_per_class, mhit_ensemble** out) {
+  if (!out || slots_per_class < 1) return MHIT_ERR_INVALID;
+  mhit_ensemble* e = new mhit_ensemble();
+  cudaGetDevice(&e->device);
+  size_t freeb = 0, total = 0;
+  if (cudaMemGetInfo(&freeb, &total) != cudaSuccess) {
+    delete e;
+    return MHIT_ERR_CUDA;
+  }
+  // default budget: 85% of the free memory
+  e->budget = hbm_budget_bytes ? hbm_budget_bytes : (size_t)(0.85 * (double)freeb);
+  e->slots_per_class = slots_per_class;
+  e->t0 = now_s();
+  *out = e;
+  return MHIT_OK;
+}
+
+int mhit_ens_submit(mhit_ensemble* e, const mhit_params* p, int n, int precision, int phase_field, int nsteps,
+                    const double* u, const double* v, const double* w, const double* phi, int keep_result,
+                    int64_t* id) {
+  if (!e || !p || !u || !v || !w || !id || nsteps < 1) return MHIT_ERR_INVALID;
+  if (phase_field && !phi) return MHIT_ERR_INVALID;
+  if (!built_size(n)) return MHIT_ERR_UNSUPPORTED;
+  if (precision != MHIT_FP64 && precision != MHIT_FP32_REFINE) return MHIT_ERR_UNSUPPORTED;
+  if (precision == MHIT_FP32_REFINE && p->k2_mode != MHIT_K2_FD) return MHIT_ERR_UNSUPPORTED;
+  if (slot_bytes(n, phase_field, precision) > e->budget) return MHIT_ERR_NOMEM;
+  std::unique_ptr<Request> r(new Request());
+  r->id = e->next_id++;
+  r->n = n;
+  r->pf = phase_field ? 1 : 0;
+  r->precision = precision;
+  r->nsteps = nsteps;
+  r->keep = keep_result ? 1 : 0;
+  r->prm = *p;
+  memset(&r->diag, 0, sizeof(r->diag));
+  const size_t N3 = (size_t)n * n * n;
+  r->in[0].assign(u, u + N3);
+  r->in[1].assign(v, v + N3);
+  r->in[2].assign(w, w + N3);
+  if (r->pf) r->in[3].assign(phi, phi + N3);
+  r->t_submit = now_s();
+  *id = r->id;
+  e->queue.push_back(r->id);
+  e->reqs[r->id] = std::move(r);
+  return MHIT_OK;
+}
+
+// One round: finish completed requests, admit queued ones, then advance every
+// class that has running slots by one step (its graph, or an autotuner trial).
+// *pending = requests queued or running after the round.
+int mhit_ens_progress(mhit_ensemble* e, int* pending) {
+  if (!e) return MHIT_ERR_INVALID;
+  int dev = -1;
+  cudaGetDevice(&dev);
+  if (dev != e->device) cudaSetDevice(e->device);
+  // 1. completions
+  for (auto& kv : e->reqs) {
+    Request* r = kv.second.get();
+    if (r->finishing && cudaEventQuery(r->done_ev) == cudaSuccess) complete(e, r);
+  }
+  // 2. admission, in arrival order, of everything that fits now
+  for (auto it = e->queue.begin(); it != e->queue.end();) {
+    Request* r = e->reqs[*it].get();
+    int err = MHIT_OK;
+    if (admit(e, r, &err)) {
+      it = e->queue.erase(it);
+    } else {
+      if (err) {
+        r->state = RQ_FAILED;
+        r->status = err;
+        r->t_done = now_s();
+        it = e->queue.erase(it);
+      } else {
+        ++it;
+      }
+    }
+  }
+  // 3. one step of every class with running slots
+  for (auto& cp : e->classes) {
+    Class* c = cp.get();
+    bool busy = false;
+    for (auto& b : c->slots)
+      if (b.req >= 0 && !e->reqs[b.req]->finishing) busy = true;
+    if (!busy) continue;
+    // at most two rounds in flight per class
+    cudaEvent_t& slot_ev = c->inflight[c->rounds & 1];
+    if (slot_ev) {
+      if (cudaEventQuery(slot_ev) != cudaSuccess) continue;
+    } else {
+      ECK(e, cudaEventCreateWithFlags(&slot_ev, cudaEventDisableTiming));
+    }
+    if (!c->tuned) {
+      // autotuner: time each z-chunk candidate on live data, twice
+      const int ci = c->tune_idx % (int)c->cand.size();
+      ECK(e, cudaEventRecord(c->ev0, c->st));
+      ECK(e, enqueue_class_step(c, c->cand[ci].first, c->cand[ci].second));
+      ECK(e, cudaEventRecord(c->ev1, c->st));
+      ECK(e, cudaEventSynchronize(c->ev1));
+      float ms = 0;
+      cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+      if (c->tune_idx >= (int)c->cand.size()) {  // first pass is warm-up
+        c->cand_ms[ci] += ms;
+        c->cand_runs[ci] += 1;
+      }
+      ++c->tune_idx;
+      if (c->tune_idx >= 3 * (int)c->cand.size()) {
+        int best = 0;
+        for (size_t q = 1; q < c->cand.size(); ++q)
+          if (c->cand_ms[q] / c->cand_runs[q] < c->cand_ms[best] / c->cand_runs[best]) best = (int)q;
+        c->kz = c->cand[best].first;
+        c->mty = c->cand[best].second;
+        ECK(e, capture_class(c, c->kz, c->mty));
+        c->tuned = true;
+      }
+    } else {
+      ECK(e, cudaGraphLaunch(c->graph, c->st));
+    }
+    ECK(e, cudaEventRecord(slot_ev, c->st));
+    ++c->rounds;
+    ++e->launches;
+    for (auto& b : c->slots) {
+      if (b.req < 0) continue;
+      Request* r = e->reqs[b.req].get();
+      if (r->finishing) continue;
+      if (++r->steps_issued >= r->nsteps) ECK(e, retire_enqueue(e, c, r));
+    }
+  }
+  ++e->rounds;
+  int pend = 0;
+  for (auto& kv : e->reqs)
+    if (kv.second->state == RQ_QUEUED || kv.second->state == RQ_RUNNING) ++pend;
+  if (pending) *pending = pend;
+  if (dev >= 0 && dev != e->device) cudaSetDevice(dev);
+  return MHIT_OK;
+}
+
+int mhit_ens_query(mhit_ensemble* e, int64_t id, mhit_ens_info* out) {
+  if (!e || !out) return MHIT_ERR_INVALID;
+  auto it = e->reqs.find(id);
+  if (it == e->reqs.end()) return MHIT_ERR_INVALID;
+  const Request* r = it->second.get();
+  memset(out, 0, sizeof(*out));
+  out->state = r->state;
+  out->status = r->status;
+  out->n = r->n;
+  out->steps_issued = r->steps_issued;
+  out->t_submit = r->t_submit - e->t0;
+  out->t_admit = r->t_admit > 0 ? r->t_admit - e->t0 : -1.0;
+  out->t_done = r->t_done > 0 ? r->t_done - e->t0 : -1.0;
+  out->diag = r->diag;
+  if (r->cls >= 0) {
+    out->kz = e->classes[r->cls]->kz;
+    out->mty = e->classes[r->cls]->mty;
+  }
+  return MHIT_OK;
+}
+
+int mhit_ens_result(mhit_ensemble* e, int64_t id, double* u, double* v, double* w, double* phi) {
+  if (!e) return MHIT_ERR_INVALID;
+  auto it = e->reqs.find(id);
+  if (it == e->reqs.end()) return MHIT_ERR_INVALID;
+  Request* r = it->second.get();
+  if (r->state != RQ_DONE && r->state != RQ_FAILED) return MHIT_ERR_STATE;
+  if (!r->keep || r->out[0].empty()) return MHIT_ERR_STATE;
+  double* dst[4] = {u, v, w, phi};
+  for (int f = 0; f < 4; ++f)
+    if (dst[f] && !r->out[f].empty()) memcpy(dst[f], r->out[f].data(), r->out[f].size() * sizeof(double));
+  return MHIT_OK;
+}
+
+// Drop a finished request's record (and its kept fields).
+int mhit_ens_release(mhit_ensemble* e, int64_t id) {
+  if (!e) return MHIT_ERR_INVALID;
+  auto it = e->reqs.find(id);
+  if (it == e->reqs.end()) return MHIT_ERR_INVALID;
+  if (it->second->state == RQ_QUEUED || it->second->state == RQ_RUNNING) return MHIT_ERR_STATE;
+  e->reqs.erase(it);
+  return MHIT_OK;
+}
+
+int mhit_ens_cancel(mhit_ensemble* e, int64_t id) {
+  if (!e) return MHIT_ERR_INVALID;
+  auto it = e->reqs.find(id);
+  if (it == e->reqs.end()) return MHIT_ERR_INVALID;
+  Request* r = it->second.get();
+  if (r->state == RQ_QUEUED) {
+    e->queue.erase(std::remove(e->queue.begin(), e->queue.end(), id), e->queue.end());
+  } else if (r->state == RQ_RUNNING) {
+    Class* c = e->classes[r->cls].get();
+    if (r->finishing) {
+      cudaEventSynchronize(r->done_ev);
+      complete(e, r);
+    } else {
+      ECK(e, set_active(c, r->slot, 0));
+      ECK(e, cudaStreamSynchronize(c->st));
+      c->slots[r->slot].req = -1;
+    }
+  } else {
+    return MHIT_OK;
+  }
+  r->state = RQ_CANCELLED;
+  r->t_done = now_s();
+  return MHIT_OK;
+}
+
+int mhit_ens_stats(mhit_ensemble* e, mhit_ens_stats_t* out) {
+  if (!e || !out) return MHIT_ERR_INVALID;
+  memset(out, 0, sizeof(*out));
+  out->rounds = e->rounds;
+  out->graph_launches = e->launches;
+  out->bytes_used = e->used;
+  out->bytes_budget = e->budget;
+  out->classes = (int)e->classes.size();
+  for (auto& c : e->classes) out->slots += c->nslots;
+  return MHIT_OK;
+}
+
+const char* mhit_ens_last_error(mhit_ensemble* e) { return e ? e->last_error.c_str() : ""; }
+
+int mhit_ens_destroy(mhit_ensemble* e) {
+  if (!e) return MHIT_ERR_INVALID;
+  for (auto& c : e->classes) cudaStreamSynchronize(c->st);
+  for (auto& kv : e->reqs) {
+    Request* r = kv.second.get();
+    if (r->done_ev) cudaEventDestroy(r->done_ev);
+    if (r->pinned) cudaFreeHost(r->pinned);
+  }
+  for (auto& c : e->classes) {
+    for (auto& b : c->slots) free_slot_buffers(e, b);
+    if (c->graph) cudaGraphExecDestroy(c->graph);
+    for (auto& ev : c->inflight)
+      if (ev) cudaEventDestroy(ev);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    cudaFree(c->d_slots);
+    cudaFree(c->d_ctrl);
+    cudaFreeHost(c->h_ctrl);
+    cudaFree(c->tw);
+    cudaFree(c->k2tab);
+    cudaStreamDestroy(c->st);
+  }
+  delete e;
+  return MHIT_OK;
+}
+
+}  // extern "C"

@@ -1,8 +1,10 @@
 // Shared-memory batched FFT for libmhit.
 //
 // A CTA holds L complex lines of length N in shared memory, interleaved so
-// that element n of line l sits at s[n*L + l] ("column-major": the L lines
-// are the fast axis).  That is the layout of a chunk of L consecutive kx
+// that element n of line l sits at s[n*LP + l] with the row pitch LP = L + 1
+// ("column-major": the L lines are the fast axis; the one-element pad per row
+// keeps both the stage accesses and x-fastest staging writes free of bank
+// conflicts).  That is the layout of a chunk of L consecutive kx
 // columns of the spectrum, so the y and z passes stage 128-byte rows straight
 // from HBM, and every Stockham stage below reads and writes 32 consecutive
 // elements per warp (no shared-memory bank conflicts for 8- or 16-byte
@@ -92,8 +94,11 @@ template <int DIR, class C> struct DFT<3, DIR, C> {
 template <class C> __device__ __forceinline__ C ldg_c(const C* p) { return __ldg(p); }
 
 // One Stockham stage over L interleaved lines, NT threads.
+template <int L> struct Pitch { static constexpr int value = L + 1; };
+
 template <int N, int R, int NS, int L, int NT, int DIR, class C>
 __device__ __forceinline__ void fft_stage(C* s, const C* __restrict__ tw) {
+  constexpr int LP = Pitch<L>::value;
   constexpr int NR = N / R;
   constexpr int W = L * NR;
   constexpr int ITEMS = (W + NT - 1) / NT;
@@ -107,7 +112,7 @@ __device__ __forceinline__ void fft_stage(C* s, const C* __restrict__ tw) {
       const int jm = j % NS;
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        C a = s[(j + r * NR) * L + l];
+        C a = s[(j + r * NR) * LP + l];
         if (NS > 1 && r > 0) {
           C t = ldg_c(tw + r * jm * TSTRIDE);
           a = (DIR < 0) ? cmul(a, t) : cmulc(a, t);
@@ -126,7 +131,7 @@ __device__ __forceinline__ void fft_stage(C* s, const C* __restrict__ tw) {
       const int jm = j % NS;
       const int d0 = (j / NS) * NS * R + jm;
 #pragma unroll
-      for (int r = 0; r < R; ++r) s[(d0 + r * NS) * L + l] = v[it][r];
+      for (int r = 0; r < R; ++r) s[(d0 + r * NS) * LP + l] = v[it][r];
     }
   }
   __syncthreads();

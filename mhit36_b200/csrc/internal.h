@@ -53,8 +53,38 @@ template <class T> struct StencilArgs {
   StepConst c;
 };
 
-template <class T> cudaError_t launch_phase(const StencilArgs<T>& a, cudaStream_t st);
-template <class T> cudaError_t launch_momentum(const StencilArgs<T>& a, bool phase_field, cudaStream_t st);
+// One resident simulation of a served ensemble: the batched kernels read
+// their arguments from a device array of these, one per slot of a class.
+template <class T> struct SlotArgs {
+  StencilArgs<T> st;    // phi_in / phi_out are chosen on the device by step parity
+  PoissonArgs<T> po;    // the Poisson solve (FP32 form: first solve -> p0)
+  PoissonArgs<T> pr;    // FP32 form: correction solve of the FP64 residual -> dp
+  T* phi[2];
+  float* dp;            // FP32 form: correction pressure
+  int active;           // 0: every kernel of this slot returns at once
+  int pad_;
+};
+
+// Batched launches over `nslots` slots of one class (grid size n).  kz is
+// the stencil kernels' z chunk (chosen by the autotuner).
+template <class T> cudaError_t launch_phase_batched(const SlotArgs<T>* slots, int nslots, int n, int kz, cudaStream_t st);
+template <class T>
+cudaError_t launch_momentum_batched(const SlotArgs<T>* slots, int nslots, int n, int kz, bool pf, cudaStream_t st,
+                                   int mty);
+template <class T> cudaError_t launch_project_batched(const SlotArgs<T>* slots, int nslots, int n, cudaStream_t st);
+cudaError_t launch_finalize_batched(const SlotArgs<double>* slots, int nslots, int n, cudaStream_t st);
+cudaError_t launch_finalize_batched_f32(const SlotArgs<float>* slots, int nslots, int n, cudaStream_t st);
+// Poisson stage (0..4) for every slot; `which` 0 = po, 1 = pr.
+template <class T>
+cudaError_t launch_poisson_stage_batched(const SlotArgs<T>* slots, int nslots, int n, int stage, int which,
+                                         cudaStream_t st);
+int stencil_kz_ok(int n, int kz);
+
+// kz: z chunk of the stencil kernels (0 = default); mty: momentum tile height (8 or 16).
+template <class T> cudaError_t launch_phase(const StencilArgs<T>& a, cudaStream_t st, int kz);
+template <class T>
+cudaError_t launch_momentum(const StencilArgs<T>& a, bool phase_field, cudaStream_t st, int kz, int mty);
+int default_mty(int n);
 template <class T> cudaError_t launch_project(const StencilArgs<T>& a, cudaStream_t st);
 // FP32 refinement form: p = p0 + dp, projection and max|div u| in FP64.
 cudaError_t launch_project_refine(const StencilArgs<float>& a, const float* dp, cudaStream_t st);
@@ -70,5 +100,9 @@ template <class T>
 cudaError_t launch_stats(const T* u, const T* v, const T* w, const T* phi, const Ctrl* ctrl, int n, double dxi_c,
                          double dxi_d, double* partials, double* out, cudaStream_t st);
 int stats_partials(int n);
+
+template <class T>
+cudaError_t launch_dropcount(const T* phi, int n, int* lab, int* cnt, int2* roots, int cap, int* d_counter,
+                             cudaStream_t st);
 
 }  // namespace mhit

@@ -16,6 +16,7 @@
 //   * The z pass fuses forward FFT, the k^2 division and the inverse FFT.
 //   * The inverse x pass is complex-to-real for two lines at once.
 #include <cuda_runtime.h>
+#include <algorithm>
 #include "common.cuh"
 #include "fft.cuh"
 #include "internal.h"
@@ -65,36 +66,38 @@ __device__ __forceinline__ double xfwd_rhs(const T* __restrict__ us, const T* __
 }
 
 template <int N, int MODE, class T>
-__global__ void __launch_bounds__(256, 3) xfwd_kernel(const T* __restrict__ us, const T* __restrict__ vs,
-                                                  const T* __restrict__ ws, const T* __restrict__ rhs,
-                                                  const T* __restrict__ p0,
-                                                  typename C2<T>::t* __restrict__ spec,
-                                                  const typename C2<T>::t* __restrict__ tw,
-                                                  const Ctrl* __restrict__ ctrl, double cdiv, double ddxi) {
+__device__ __forceinline__ void xfwd_body(const T* __restrict__ us, const T* __restrict__ vs,
+                                          const T* __restrict__ ws, const T* __restrict__ rhs,
+                                          const T* __restrict__ p0, typename C2<T>::t* __restrict__ spec,
+                                          const typename C2<T>::t* __restrict__ tw, const Ctrl* __restrict__ ctrl,
+                                          double cdiv, double ddxi, int bx, int by) {
   typedef typename C2<T>::t C;
   typedef PCfg<N> G;
   constexpr int P = G::P, NT = G::NT;
   if (ctrl && ctrl->status) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* s = reinterpret_cast<C*>(smem_raw);
-  const int j0 = blockIdx.x * (2 * P);
-  const int k = blockIdx.y;
+  constexpr int LP = Pitch<P>::value;
+  const int j0 = bx * (2 * P);
+  const int k = by;
+  // x-fastest: each warp reads 32 consecutive cells of the same lines
   for (int wi = threadIdx.x; wi < P * N; wi += NT) {
-    const int p = wi % P, n = wi / P;
+    const int n = wi % N, p = wi / N;
     const int ja = j0 + 2 * p;
     C z;
     z.x = (T)xfwd_rhs<N, MODE, T>(us, vs, ws, rhs, p0, cdiv, ddxi, n, ja, k);
     z.y = (T)xfwd_rhs<N, MODE, T>(us, vs, ws, rhs, p0, cdiv, ddxi, n, ja + 1, k);
-    s[n * P + p] = z;
+    s[n * LP + p] = z;
   }
   __syncthreads();
   smem_fft<N, P, NT, -1>(s, tw);
   const T half = (T)0.5;
-  for (int wi = threadIdx.x; wi < P * (N / 2 + 1); wi += NT) {
-    const int p = wi % P, m = wi / P;
+  constexpr int M = N / 2 + 1;
+  for (int wi = threadIdx.x; wi < P * M; wi += NT) {
+    const int m = wi % M, p = wi / M;
     const int ja = j0 + 2 * p;
-    const C zm = s[m * P + p];
-    const C zr = s[((m == 0) ? 0 : (N - m)) * P + p];
+    const C zm = s[m * LP + p];
+    const C zr = s[((m == 0) ? 0 : (N - m)) * LP + p];
     C A, B;
     A.x = half * (zm.x + zr.x);
     A.y = half * (zm.y - zr.y);
@@ -108,25 +111,26 @@ __global__ void __launch_bounds__(256, 3) xfwd_kernel(const T* __restrict__ us, 
 
 // ---------------------------------------------------------------- y pass
 template <int N, int DIR, class T>
-__global__ void __launch_bounds__(256, 3) ypass_kernel(typename C2<T>::t* __restrict__ spec,
-                                                   const typename C2<T>::t* __restrict__ tw,
-                                                   const Ctrl* __restrict__ ctrl) {
+__device__ __forceinline__ void ypass_body(typename C2<T>::t* __restrict__ spec,
+                                           const typename C2<T>::t* __restrict__ tw, const Ctrl* __restrict__ ctrl,
+                                           int bx, int by) {
   typedef typename C2<T>::t C;
   typedef PCfg<N> G;
   constexpr int CC = G::CC, NT = G::NT;
   if (ctrl && ctrl->status) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* s = reinterpret_cast<C*>(smem_raw);
-  C* base = spec + (size_t)blockIdx.y * N * G::PITCH + blockIdx.x * CC;
+  C* base = spec + (size_t)by * N * G::PITCH + bx * CC;
+  constexpr int LP = Pitch<CC>::value;
   for (int wi = threadIdx.x; wi < CC * N; wi += NT) {
     const int l = wi % CC, n = wi / CC;
-    s[wi] = base[(size_t)n * G::PITCH + l];
+    s[n * LP + l] = base[(size_t)n * G::PITCH + l];
   }
   __syncthreads();
   smem_fft<N, CC, NT, DIR>(s, tw);
   for (int wi = threadIdx.x; wi < CC * N; wi += NT) {
     const int l = wi % CC, n = wi / CC;
-    base[(size_t)n * G::PITCH + l] = s[wi];
+    base[(size_t)n * G::PITCH + l] = s[n * LP + l];
   }
 }
 
@@ -135,23 +139,24 @@ __global__ void __launch_bounds__(256, 3) ypass_kernel(typename C2<T>::t* __rest
 // (multi/main.f90:785-798), inverse z FFT, all in shared memory.
 // k2tab[m] holds kx(m)^2 (spectral) or (4/dx^2) sin^2(pi m/N) (FD-modified).
 template <int N, class T>
-__global__ void __launch_bounds__(256, 3) zsolve_kernel(typename C2<T>::t* __restrict__ spec,
-                                                    const typename C2<T>::t* __restrict__ tw,
-                                                    const double* __restrict__ k2tab,
-                                                    const Ctrl* __restrict__ ctrl) {
+__device__ __forceinline__ void zsolve_body(typename C2<T>::t* __restrict__ spec,
+                                            const typename C2<T>::t* __restrict__ tw,
+                                            const double* __restrict__ k2tab, const Ctrl* __restrict__ ctrl, int bx,
+                                            int by) {
   typedef typename C2<T>::t C;
   typedef PCfg<N> G;
   constexpr int CC = G::CC, NT = G::NT;
   if (ctrl && ctrl->status) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* s = reinterpret_cast<C*>(smem_raw);
-  const int jy = blockIdx.y;
-  const int m0 = blockIdx.x * CC;
+  const int jy = by;
+  const int m0 = bx * CC;
   C* base = spec + (size_t)jy * G::PITCH + m0;
   const size_t zstride = (size_t)N * G::PITCH;
+  constexpr int LP = Pitch<CC>::value;
   for (int wi = threadIdx.x; wi < CC * N; wi += NT) {
     const int l = wi % CC, n = wi / CC;
-    s[wi] = base[(size_t)n * zstride + l];
+    s[n * LP + l] = base[(size_t)n * zstride + l];
   }
   __syncthreads();
   smem_fft<N, CC, NT, -1>(s, tw);
@@ -160,42 +165,192 @@ __global__ void __launch_bounds__(256, 3) zsolve_kernel(typename C2<T>::t* __res
   for (int wi = threadIdx.x; wi < CC * N; wi += NT) {
     const int l = wi % CC, n = wi / CC;
     const int m = m0 + l;
-    C v = s[wi];
+    C v = s[n * LP + l];
     if (m > N / 2 || (m == 0 && jy == 0 && n == 0)) {
       v.x = 0;
       v.y = 0;
     } else {
       const double k2 = (k2tab[m] + k2y) + k2tab[n];
-      v.x = (T)(-(double)v.x / k2 / nnn);
-      v.y = (T)(-(double)v.y / k2 / nnn);
+      const double f = -1.0 / (k2 * nnn);
+      v.x = (T)((double)v.x * f);
+      v.y = (T)((double)v.y * f);
     }
-    s[wi] = v;
+    s[n * LP + l] = v;
   }
   __syncthreads();
   smem_fft<N, CC, NT, +1>(s, tw);
   for (int wi = threadIdx.x; wi < CC * N; wi += NT) {
     const int l = wi % CC, n = wi / CC;
-    base[(size_t)n * zstride + l] = s[wi];
+    base[(size_t)n * zstride + l] = s[n * LP + l];
   }
+}
+
+// ---------------------------------------------------------------- persistent column passes
+// The y passes and the z solve as persistent kernels: each CTA walks a
+// strided list of (column chunk, line) slabs.  The slab after the current one
+// is copied into the second shared-memory buffer with cp.async while the
+// current one is transformed, so HBM traffic overlaps the FFT arithmetic.
+// KIND 0/1: y pass forward/inverse; KIND 2: z solve.
+struct ColSlab {
+  void* spec;        // slab base (the chunk's first element)
+  size_t stride;     // distance between consecutive elements of a column (complex)
+  const void* tw;
+  const double* k2tab;
+  int jy;            // z solve: the ky index of the slab
+  int m0;            // z solve: first kx of the chunk
+  bool live;         // false: skip (inactive slot or stopped simulation)
+};
+
+template <int N, int KIND, class T>
+__device__ __forceinline__ void colpass_issue(typename C2<T>::t* buf, const ColSlab& sl) {
+  typedef typename C2<T>::t C;
+  typedef PCfg<N> G;
+  constexpr int CC = G::CC, NT = G::NT, LP = Pitch<CC>::value;
+  if (sl.live) {
+    const C* base = static_cast<const C*>(sl.spec);
+    for (int wi = threadIdx.x; wi < CC * N; wi += NT) {
+      const int l = wi % CC, n = wi / CC;
+      cp_async_elem(buf + n * LP + l, base + (size_t)n * sl.stride + l);
+    }
+  }
+  cp_async_commit();
+}
+
+template <int N, int KIND, class T>
+__device__ __forceinline__ void colpass_compute(typename C2<T>::t* s, const ColSlab& sl) {
+  typedef typename C2<T>::t C;
+  typedef PCfg<N> G;
+  constexpr int CC = G::CC, NT = G::NT, LP = Pitch<CC>::value;
+  const C* tw = static_cast<const C*>(sl.tw);
+  if (KIND == 0) {
+    smem_fft<N, CC, NT, -1>(s, tw);
+  } else if (KIND == 1) {
+    smem_fft<N, CC, NT, +1>(s, tw);
+  } else {
+    smem_fft<N, CC, NT, -1>(s, tw);
+    const double nnn = (double)((long long)N * (long long)N * (long long)N);
+    const double k2y = sl.k2tab[sl.jy];
+    for (int wi = threadIdx.x; wi < CC * N; wi += NT) {
+      const int l = wi % CC, n = wi / CC;
+      const int m = sl.m0 + l;
+      C v = s[n * LP + l];
+      if (m > N / 2 || (m == 0 && sl.jy == 0 && n == 0)) {
+        v.x = 0;
+        v.y = 0;
+      } else {
+        // -psi/k2/(nx*ny*nz) (multi/main.f90:792) as one reciprocal per mode
+        const double k2 = (sl.k2tab[m] + k2y) + sl.k2tab[n];
+        const double f = -1.0 / (k2 * nnn);
+        v.x = (T)((double)v.x * f);
+        v.y = (T)((double)v.y * f);
+      }
+      s[n * LP + l] = v;
+    }
+    __syncthreads();
+    smem_fft<N, CC, NT, +1>(s, tw);
+  }
+  C* base = static_cast<C*>(sl.spec);
+  for (int wi = threadIdx.x; wi < CC * N; wi += NT) {
+    const int l = wi % CC, n = wi / CC;
+    base[(size_t)n * sl.stride + l] = s[n * LP + l];
+  }
+}
+
+// Slab `it` of a single simulation.
+template <int N, int KIND, class T>
+__device__ __forceinline__ ColSlab slab_single(typename C2<T>::t* spec, const void* tw, const double* k2tab,
+                                               const Ctrl* ctrl, int it) {
+  typedef PCfg<N> G;
+  ColSlab sl;
+  const int chunk = it % G::NCHUNK, line = it / G::NCHUNK;
+  sl.live = !(ctrl && ctrl->status);
+  sl.tw = tw;
+  sl.k2tab = k2tab;
+  sl.m0 = chunk * G::CC;
+  if (KIND == 2) {
+    sl.spec = spec + (size_t)line * G::PITCH + chunk * G::CC;
+    sl.stride = (size_t)N * G::PITCH;
+    sl.jy = line;
+  } else {
+    sl.spec = spec + (size_t)line * N * G::PITCH + chunk * G::CC;
+    sl.stride = G::PITCH;
+    sl.jy = 0;
+  }
+  return sl;
+}
+
+template <int N, int KIND, class T, class Getter>
+__device__ __forceinline__ void colpass_run(int total, Getter get) {
+  typedef typename C2<T>::t C;
+  typedef PCfg<N> G;
+  constexpr int LP = Pitch<G::CC>::value;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* buf0 = reinterpret_cast<C*>(smem_raw);
+  C* buf1 = buf0 + N * LP;
+  int it = blockIdx.x;
+  if (it >= total) return;
+  ColSlab cur = get(it);
+  colpass_issue<N, KIND, T>(buf0, cur);
+  for (int t = 0; it < total; ++t) {
+    const int nxt = it + gridDim.x;
+    ColSlab next;
+    next.live = false;
+    if (nxt < total) next = get(nxt);
+    colpass_issue<N, KIND, T>((t & 1) ? buf0 : buf1, next);
+    cp_async_wait<1>();
+    __syncthreads();
+    if (cur.live) colpass_compute<N, KIND, T>((t & 1) ? buf1 : buf0, cur);
+    __syncthreads();
+    it = nxt;
+    cur = next;
+  }
+}
+
+template <int N, int KIND, class T>
+__global__ void __launch_bounds__(256, 2) colpass_kernel(typename C2<T>::t* __restrict__ spec,
+                                                     const typename C2<T>::t* __restrict__ tw,
+                                                     const double* __restrict__ k2tab, const Ctrl* __restrict__ ctrl) {
+  typedef PCfg<N> G;
+  colpass_run<N, KIND, T>(G::NCHUNK * N, [&](int it) { return slab_single<N, KIND, T>(spec, tw, k2tab, ctrl, it); });
+}
+
+template <int N, int KIND, class T>
+__global__ void __launch_bounds__(256, 2) colpass_kernel_b(const SlotArgs<T>* __restrict__ slots, int nslots,
+                                                       int which) {
+  typedef PCfg<N> G;
+  const int per = G::NCHUNK * N;
+  colpass_run<N, KIND, T>(per * nslots, [&](int it) {
+    const int sl = it / per;
+    const PoissonArgs<T>& a = which ? slots[sl].pr : slots[sl].po;
+    ColSlab s;
+    if (!slots[sl].active) {
+      s.live = false;
+      return s;
+    }
+    s = slab_single<N, KIND, T>(a.spec, a.tw, a.k2tab, a.ctrl, it - sl * per);
+    return s;
+  });
 }
 
 // ---------------------------------------------------------------- x inverse
 // Complex-to-real x transform of two lines at once; writes p
 // (multi/main.f90:812, 842-850: p = real(psi)).
 template <int N, class T>
-__global__ void __launch_bounds__(256, 3) xinv_kernel(const typename C2<T>::t* __restrict__ spec, T* __restrict__ p,
-                                                  const typename C2<T>::t* __restrict__ tw,
-                                                  const Ctrl* __restrict__ ctrl) {
+__device__ __forceinline__ void xinv_body(const typename C2<T>::t* __restrict__ spec, T* __restrict__ p,
+                                          const typename C2<T>::t* __restrict__ tw, const Ctrl* __restrict__ ctrl,
+                                          int bx, int by) {
   typedef typename C2<T>::t C;
   typedef PCfg<N> G;
   constexpr int P = G::P, NT = G::NT;
   if (ctrl && ctrl->status) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* s = reinterpret_cast<C*>(smem_raw);
-  const int j0 = blockIdx.x * (2 * P);
-  const int k = blockIdx.y;
-  for (int wi = threadIdx.x; wi < P * (N / 2 + 1); wi += NT) {
-    const int q = wi % P, m = wi / P;
+  constexpr int LP = Pitch<P>::value;
+  constexpr int M = N / 2 + 1;
+  const int j0 = bx * (2 * P);
+  const int k = by;
+  for (int wi = threadIdx.x; wi < P * M; wi += NT) {
+    const int m = wi % M, q = wi / M;
     const C* row = spec + ((size_t)k * N + j0 + 2 * q) * G::PITCH;
     C A = row[m];
     C B = row[G::PITCH + m];
@@ -206,28 +361,113 @@ __global__ void __launch_bounds__(256, 3) xinv_kernel(const typename C2<T>::t* _
     C z;
     z.x = A.x - B.y;
     z.y = A.y + B.x;
-    s[m * P + q] = z;
+    s[m * LP + q] = z;
     if (m > 0 && m < N / 2) {
       C zc;
       zc.x = A.x + B.y;
       zc.y = B.x - A.y;
-      s[(N - m) * P + q] = zc;
+      s[(N - m) * LP + q] = zc;
     }
   }
   __syncthreads();
   smem_fft<N, P, NT, +1>(s, tw);
   for (int wi = threadIdx.x; wi < P * N; wi += NT) {
-    const int q = wi % P, n = wi / P;
+    const int n = wi % N, q = wi / N;
     const int ja = j0 + 2 * q;
-    const C z = s[n * P + q];
+    const C z = s[n * LP + q];
     p[gidx(n, ja, k, N)] = z.x;
     p[gidx(n, ja + 1, k, N)] = z.y;
   }
 }
 
+// ---------------------------------------------------------------- entry points
+// Single solve: block coordinates are the grid's.
+template <int N, int MODE, class T>
+__global__ void __launch_bounds__(256, 3) xfwd_kernel(const T* __restrict__ us, const T* __restrict__ vs,
+                                                  const T* __restrict__ ws, const T* __restrict__ rhs,
+                                                  const T* __restrict__ p0, typename C2<T>::t* __restrict__ spec,
+                                                  const typename C2<T>::t* __restrict__ tw,
+                                                  const Ctrl* __restrict__ ctrl, double cdiv, double ddxi) {
+  xfwd_body<N, MODE, T>(us, vs, ws, rhs, p0, spec, tw, ctrl, cdiv, ddxi, blockIdx.x, blockIdx.y);
+}
+template <int N, int DIR, class T>
+__global__ void __launch_bounds__(256, 3) ypass_kernel(typename C2<T>::t* __restrict__ spec,
+                                                   const typename C2<T>::t* __restrict__ tw,
+                                                   const Ctrl* __restrict__ ctrl) {
+  ypass_body<N, DIR, T>(spec, tw, ctrl, blockIdx.x, blockIdx.y);
+}
+template <int N, class T>
+__global__ void __launch_bounds__(256, 3) zsolve_kernel(typename C2<T>::t* __restrict__ spec,
+                                                    const typename C2<T>::t* __restrict__ tw,
+                                                    const double* __restrict__ k2tab, const Ctrl* __restrict__ ctrl) {
+  zsolve_body<N, T>(spec, tw, k2tab, ctrl, blockIdx.x, blockIdx.y);
+}
+template <int N, class T>
+__global__ void __launch_bounds__(256, 3) xinv_kernel(const typename C2<T>::t* __restrict__ spec, T* __restrict__ p,
+                                                  const typename C2<T>::t* __restrict__ tw,
+                                                  const Ctrl* __restrict__ ctrl) {
+  xinv_body<N, T>(spec, p, tw, ctrl, blockIdx.x, blockIdx.y);
+}
+
+// Batched over the slots of a served ensemble: grid y = slot * N + plane.
+// `which` selects the slot's first (0) or correction (1) solve.
+template <int N, int MODE, class T>
+__global__ void __launch_bounds__(256, 3) xfwd_kernel_b(const SlotArgs<T>* __restrict__ slots, int which) {
+  const int sl = blockIdx.y / N;
+  if (!slots[sl].active) return;
+  const PoissonArgs<T>& a = which ? slots[sl].pr : slots[sl].po;
+  xfwd_body<N, MODE, T>(a.us, a.vs, a.ws, a.rhs, a.pres, a.spec, a.tw, a.ctrl, a.cdiv, a.ddxi, blockIdx.x,
+                        blockIdx.y - sl * N);
+}
+template <int N, int DIR, class T>
+__global__ void __launch_bounds__(256, 3) ypass_kernel_b(const SlotArgs<T>* __restrict__ slots, int which) {
+  const int sl = blockIdx.y / N;
+  if (!slots[sl].active) return;
+  const PoissonArgs<T>& a = which ? slots[sl].pr : slots[sl].po;
+  ypass_body<N, DIR, T>(a.spec, a.tw, a.ctrl, blockIdx.x, blockIdx.y - sl * N);
+}
+template <int N, class T>
+__global__ void __launch_bounds__(256, 3) zsolve_kernel_b(const SlotArgs<T>* __restrict__ slots, int which) {
+  const int sl = blockIdx.y / N;
+  if (!slots[sl].active) return;
+  const PoissonArgs<T>& a = which ? slots[sl].pr : slots[sl].po;
+  zsolve_body<N, T>(a.spec, a.tw, a.k2tab, a.ctrl, blockIdx.x, blockIdx.y - sl * N);
+}
+template <int N, class T>
+__global__ void __launch_bounds__(256, 3) xinv_kernel_b(const SlotArgs<T>* __restrict__ slots, int which) {
+  const int sl = blockIdx.y / N;
+  if (!slots[sl].active) return;
+  const PoissonArgs<T>& a = which ? slots[sl].pr : slots[sl].po;
+  xinv_body<N, T>(a.spec, a.p, a.tw, a.ctrl, blockIdx.x, blockIdx.y - sl * N);
+}
+
 // ---------------------------------------------------------------- launchers
-template <int N, class T> static size_t xsmem() { return (size_t)N * PCfg<N>::P * sizeof(typename C2<T>::t); }
-template <int N, class T> static size_t csmem() { return (size_t)N * PCfg<N>::CC * sizeof(typename C2<T>::t); }
+template <int N, class T> static size_t xsmem() {
+  return (size_t)N * Pitch<PCfg<N>::P>::value * sizeof(typename C2<T>::t);
+}
+template <int N, class T> static size_t csmem() {
+  return (size_t)N * Pitch<PCfg<N>::CC>::value * sizeof(typename C2<T>::t);
+}
+
+template <int N, class T> static size_t colsmem() {
+  return 2 * (size_t)N * Pitch<PCfg<N>::CC>::value * sizeof(typename C2<T>::t);
+}
+
+// Persistent grid: resident CTAs per SM (occupancy) times the SM count.
+template <int N, int KIND, class T, bool BATCHED> static int colgrid() {
+  static int grid = 0;
+  if (!grid) {
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (BATCHED)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, colpass_kernel_b<N, KIND, T>, 256, colsmem<N, T>());
+    else
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, colpass_kernel<N, KIND, T>, 256, colsmem<N, T>());
+    grid = std::max(1, sms) * std::max(1, per);
+  }
+  return grid;
+}
 
 template <int N, class T> static cudaError_t set_attrs() {
   cudaError_t e;
@@ -239,6 +479,19 @@ template <int N, class T> static cudaError_t set_attrs() {
   if ((e = cudaFuncSetAttribute(ypass_kernel<N, -1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, cs))) return e;
   if ((e = cudaFuncSetAttribute(ypass_kernel<N, 1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, cs))) return e;
   if ((e = cudaFuncSetAttribute(zsolve_kernel<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, cs))) return e;
+  if ((e = cudaFuncSetAttribute(xfwd_kernel_b<N, 0, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, xs))) return e;
+  if ((e = cudaFuncSetAttribute(xfwd_kernel_b<N, 2, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, xs))) return e;
+  if ((e = cudaFuncSetAttribute(xinv_kernel_b<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, xs))) return e;
+  if ((e = cudaFuncSetAttribute(ypass_kernel_b<N, -1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, cs))) return e;
+  if ((e = cudaFuncSetAttribute(ypass_kernel_b<N, 1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, cs))) return e;
+  if ((e = cudaFuncSetAttribute(zsolve_kernel_b<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, cs))) return e;
+  const int ps = (int)colsmem<N, T>();
+  if ((e = cudaFuncSetAttribute(colpass_kernel<N, 0, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps))) return e;
+  if ((e = cudaFuncSetAttribute(colpass_kernel<N, 1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps))) return e;
+  if ((e = cudaFuncSetAttribute(colpass_kernel<N, 2, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps))) return e;
+  if ((e = cudaFuncSetAttribute(colpass_kernel_b<N, 0, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps))) return e;
+  if ((e = cudaFuncSetAttribute(colpass_kernel_b<N, 1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps))) return e;
+  if ((e = cudaFuncSetAttribute(colpass_kernel_b<N, 2, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps))) return e;
   return cudaSuccess;
 }
 
@@ -263,10 +516,13 @@ static cudaError_t poisson_run(const PoissonArgs<T>& a, cudaStream_t st) {
   typedef PCfg<N> G;
   const dim3 gx(N / (2 * G::P), N), gc(G::NCHUNK, N);
   const size_t xs = xsmem<N, T>(), cs = csmem<N, T>();
+  (void)gc;
+  (void)cs;
+  const size_t ps = colsmem<N, T>();
   launch_xfwd<N, T>(a, st);
-  ypass_kernel<N, -1, T><<<gc, G::NT, cs, st>>>(a.spec, a.tw, a.ctrl);
-  zsolve_kernel<N, T><<<gc, G::NT, cs, st>>>(a.spec, a.tw, a.k2tab, a.ctrl);
-  ypass_kernel<N, 1, T><<<gc, G::NT, cs, st>>>(a.spec, a.tw, a.ctrl);
+  colpass_kernel<N, 0, T><<<colgrid<N, 0, T, false>(), G::NT, ps, st>>>(a.spec, a.tw, a.k2tab, a.ctrl);
+  colpass_kernel<N, 2, T><<<colgrid<N, 2, T, false>(), G::NT, ps, st>>>(a.spec, a.tw, a.k2tab, a.ctrl);
+  colpass_kernel<N, 1, T><<<colgrid<N, 1, T, false>(), G::NT, ps, st>>>(a.spec, a.tw, a.k2tab, a.ctrl);
   xinv_kernel<N, T><<<gx, G::NT, xs, st>>>(a.spec, a.p, a.tw, a.ctrl);
   return cudaGetLastError();
 }
@@ -278,9 +534,18 @@ static cudaError_t poisson_stage(const PoissonArgs<T>& a, int stage, cudaStream_
   const size_t xs = xsmem<N, T>(), cs = csmem<N, T>();
   switch (stage) {
     case 0: launch_xfwd<N, T>(a, st); break;
-    case 1: ypass_kernel<N, -1, T><<<gc, G::NT, cs, st>>>(a.spec, a.tw, a.ctrl); break;
-    case 2: zsolve_kernel<N, T><<<gc, G::NT, cs, st>>>(a.spec, a.tw, a.k2tab, a.ctrl); break;
-    case 3: ypass_kernel<N, 1, T><<<gc, G::NT, cs, st>>>(a.spec, a.tw, a.ctrl); break;
+    case 1:
+      colpass_kernel<N, 0, T><<<colgrid<N, 0, T, false>(), G::NT, colsmem<N, T>(), st>>>(a.spec, a.tw, a.k2tab,
+                                                                                       a.ctrl);
+      break;
+    case 2:
+      colpass_kernel<N, 2, T><<<colgrid<N, 2, T, false>(), G::NT, colsmem<N, T>(), st>>>(a.spec, a.tw, a.k2tab,
+                                                                                       a.ctrl);
+      break;
+    case 3:
+      colpass_kernel<N, 1, T><<<colgrid<N, 1, T, false>(), G::NT, colsmem<N, T>(), st>>>(a.spec, a.tw, a.k2tab,
+                                                                                       a.ctrl);
+      break;
     case 4: xinv_kernel<N, T><<<gx, G::NT, xs, st>>>(a.spec, a.p, a.tw, a.ctrl); break;
     default: return cudaErrorInvalidValue;
   }
@@ -301,6 +566,44 @@ cudaError_t launch_poisson_stage(int n, const PoissonArgs<T>& a, int stage, cuda
 }
 template cudaError_t launch_poisson_stage<double>(int, const PoissonArgs<double>&, int, cudaStream_t);
 template cudaError_t launch_poisson_stage<float>(int, const PoissonArgs<float>&, int, cudaStream_t);
+
+template <int N, class T>
+static cudaError_t poisson_stage_b(const SlotArgs<T>* slots, int nslots, int stage, int which, cudaStream_t st) {
+  typedef PCfg<N> G;
+  const dim3 gx(N / (2 * G::P), N * nslots), gc(G::NCHUNK, N * nslots);
+  const size_t xs = xsmem<N, T>(), cs = csmem<N, T>();
+  switch (stage) {
+    case 0:
+      if (which)
+        xfwd_kernel_b<N, 2, T><<<gx, G::NT, xs, st>>>(slots, 1);
+      else
+        xfwd_kernel_b<N, 0, T><<<gx, G::NT, xs, st>>>(slots, 0);
+      break;
+    case 1: colpass_kernel_b<N, 0, T><<<colgrid<N, 0, T, true>(), G::NT, colsmem<N, T>(), st>>>(slots, nslots, which); break;
+    case 2: colpass_kernel_b<N, 2, T><<<colgrid<N, 2, T, true>(), G::NT, colsmem<N, T>(), st>>>(slots, nslots, which); break;
+    case 3: colpass_kernel_b<N, 1, T><<<colgrid<N, 1, T, true>(), G::NT, colsmem<N, T>(), st>>>(slots, nslots, which); break;
+    case 4: xinv_kernel_b<N, T><<<gx, G::NT, xs, st>>>(slots, which); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t launch_poisson_stage_batched(const SlotArgs<T>* slots, int nslots, int n, int stage, int which,
+                                         cudaStream_t st) {
+  if ((long long)n * nslots > 65535) return cudaErrorInvalidConfiguration;
+  switch (n) {
+#define MHIT_CASE(NN) \
+  case NN:            \
+    return poisson_stage_b<NN, T>(slots, nslots, stage, which, st);
+    MHIT_FOR_SIZES(MHIT_CASE)
+#undef MHIT_CASE
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+template cudaError_t launch_poisson_stage_batched<double>(const SlotArgs<double>*, int, int, int, int, cudaStream_t);
+template cudaError_t launch_poisson_stage_batched<float>(const SlotArgs<float>*, int, int, int, int, cudaStream_t);
 
 // Opt the kernels of size n into their dynamic shared memory (once per
 // device and size; must precede graph capture).

@@ -25,6 +25,10 @@ constexpr int TX = 32, TY = 8, NT = TX * TY;
 
 static int pick_kz(int n) { return n >= 32 ? 32 : n; }
 
+// Momentum tile height (measured on B200 at 256^3 and 512^3 with the
+// one-plane cp.async prefetch: 8 rows beat 16 by 20% at both sizes).
+int default_mty(int n) { return n > 0 ? 8 : 8; }
+
 // ============================================================ phase field
 // ACDI step A1..A7 (multi/main.f90:341-480) fused into one kernel:
 //   psi = eps*log((min(phi,1)+enum)/(1-min(phi,1)+enum))      (A3)
@@ -38,7 +42,7 @@ constexpr int PTY = 16;            // phase tile height
 constexpr int PNT = TX * PTY;       // phase threads per CTA
 
 template <class T>
-__global__ void __launch_bounds__(PNT, 2) phase_kernel(StencilArgs<T> a, int KZ) {
+__device__ __forceinline__ void phase_body(const StencilArgs<T>& a, int KZ, int bx, int by, int bz) {
   if (a.ctrl->status) return;
   constexpr int TY = PTY, NT = PNT;
   constexpr int EX = TX + 4, EY = TY + 4, PE = EX * EY;
@@ -55,7 +59,11 @@ __global__ void __launch_bounds__(PNT, 2) phase_kernel(StencilArgs<T> a, int KZ)
   const int use_ident = a.c.tanh_identity;
   const T floor0 = a.c.phi_floor ? (T)0 : (T)-INFINITY;
   const T inv12e = (T)1 / ((T)1 + (T)2 * enumv);
-  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, k0 = blockIdx.z * KZ;
+  // psi where min(phi,1) is exactly 0 (far field) or 1 (drop interiors): the
+  // same expression evaluated once, so skipping the log there changes nothing.
+  const T psi0 = eps * log(((T)0 + enumv) / ((T)1 - (T)0 + enumv));
+  const T psi1 = eps * log(((T)1 + enumv) / ((T)1 - (T)1 + enumv));
+  const int x0 = bx * TX, y0 = by * TY, k0 = bz * KZ;
   const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
   const int i = x0 + tx, j = y0 + ty;
   const int ip = (i + 1 == n) ? 0 : i + 1, jp = (j + 1 == n) ? 0 : j + 1;
@@ -78,13 +86,26 @@ __global__ void __launch_bounds__(PNT, 2) phase_kernel(StencilArgs<T> a, int KZ)
     if (m + 1 <= k0 + KZ + 1) issue(m + 1);
     else cp_async_commit();
     cp_async_wait<1>();  // this thread's copies of plane m have landed
+    // velocities of the output plane k = m-2, loaded now so that their latency
+    // hides behind the psi and F work below
+    T uc = 0, uxp = 0, vc = 0, vyp = 0, wc = 0, wzp = 0;
+    if (m >= k0 + 2) {
+      const int kz = wrapi(m - 2, n), kzp = wrapi(m - 1, n);
+      const size_t g = (size_t)i + (size_t)n * j + nn * kz;
+      uc = a.u[g];
+      uxp = a.u[(size_t)ip + (size_t)n * j + nn * kz];
+      vc = a.v[g];
+      vyp = a.v[(size_t)i + (size_t)n * jp + nn * kz];
+      wc = a.w[g];
+      wzp = a.w[(size_t)i + (size_t)n * j + nn * kzp];
+    }
     // (1) psi of plane m on the elements this thread copied.
     {
       const T* Pphi = s_phi + ((m + 15) % 5) * PE;
       T* Ppsi = s_psi + ((m + 15) % 3) * PE;
       for (int e = tid; e < PE; e += NT) {
         const T val = fmax(fmin(Pphi[e], (T)1), floor0);
-        Ppsi[e] = eps * log((val + enumv) / ((T)1 - val + enumv));
+        Ppsi[e] = (val == (T)0) ? psi0 : ((val == (T)1) ? psi1 : eps * log((val + enumv) / ((T)1 - val + enumv)));
       }
     }
     __syncthreads();
@@ -102,6 +123,12 @@ __global__ void __launch_bounds__(PNT, 2) phase_kernel(StencilArgs<T> a, int KZ)
         const T gxv = Pc[pe + 1] - Pc[pe - 1];
         const T gyv = Pc[pe + EX] - Pc[pe - EX];
         const T gzv = Pp[pe] - Pm[pe];
+        if (gxv == (T)0 && gyv == (T)0 && gzv == (T)0) {  // uniform psi: n = 0 and F = 0 exactly
+          F[e] = (T)0;
+          F[FE + e] = (T)0;
+          F[2 * FE + e] = (T)0;
+          continue;
+        }
         const T normod = (T)1 / (sqrt(gxv * gxv + gyv * gyv + gzv * gzv) + tiny);
         T t;
         if (use_ident) {
@@ -121,7 +148,7 @@ __global__ void __launch_bounds__(PNT, 2) phase_kernel(StencilArgs<T> a, int KZ)
     // (3) output plane k = m-2.
     if (m >= k0 + 2) {
       const int k = m - 2;
-      const int kz = wrapi(k, n), kzp = wrapi(k + 1, n);
+      const int kz = wrapi(k, n);
       const T* P0 = s_phi + ((k + 15) % 5) * PE;
       const T* Pm1 = s_phi + ((k + 14) % 5) * PE;
       const T* Pp1 = s_phi + ((k + 16) % 5) * PE;
@@ -133,9 +160,7 @@ __global__ void __launch_bounds__(PNT, 2) phase_kernel(StencilArgs<T> a, int KZ)
       const T c = P0[pe], pxp = P0[pe + 1], pxm = P0[pe - 1], pyp = P0[pe + EX], pym = P0[pe - EX];
       const T pzp = Pp1[pe], pzm = Pm1[pe];
       const size_t g = (size_t)i + (size_t)n * j + nn * kz;
-      const T uc = a.u[g] - mu, uxp = a.u[(size_t)ip + (size_t)n * j + nn * kz] - mu;
-      const T vc = a.v[g] - mv, vyp = a.v[(size_t)i + (size_t)n * jp + nn * kz] - mv;
-      const T wc = a.w[g] - mw, wzp = a.w[(size_t)i + (size_t)n * j + nn * kzp] - mw;
+      uc -= mu; uxp -= mu; vc -= mv; vyp -= mv; wc -= mw; wzp -= mw;
       const T h = (T)0.5;
       T r = -(uxp * h * (pxp + c) - uc * h * (c + pxm)) * dxi - (vyp * h * (pyp + c) - vc * h * (c + pym)) * dxi -
             (wzp * h * (pzp + c) - wc * h * (c + pzm)) * dxi;
@@ -154,9 +179,11 @@ __global__ void __launch_bounds__(PNT, 2) phase_kernel(StencilArgs<T> a, int KZ)
 // f = 6 sigma chempot grad(phi) at cell centres interpolated to the faces,
 // and the AB2 (Euler on the first step) predictor.  Writes ustar and the new
 // rhs_o; reads the NEW phi (the reference computes B4 after A7).
-template <class T, bool PF>
-__global__ void __launch_bounds__(NT) momentum_kernel(StencilArgs<T> a, int KZ) {
+// momentum tile height: 8 or 16 rows (a tuning choice per grid size)
+template <class T, bool PF, int MTYv>
+__device__ __forceinline__ void momentum_body(const StencilArgs<T>& a, int KZ, int bx, int by, int bz) {
   if (a.ctrl->status) return;
+  constexpr int TY = MTYv, NT = TX * MTYv;
   constexpr int UX = TX + 2, UY = TY + 2, UE = UX * UY;  // velocity planes, 1-cell ring
   constexpr int EX = TX + 4, EY = TY + 4, PE = EX * EY;  // phi planes, 2-cell ring
   constexpr int QX = TX + 1, QY = TY + 1, QE = QX * QY;  // force over [-1,TX) x [-1,TY)
@@ -172,7 +199,7 @@ __global__ void __launch_bounds__(NT) momentum_kernel(StencilArgs<T> a, int KZ) 
   const T f1 = (T)a.c.f1, f2 = (T)a.c.f2, f3 = (T)a.c.f3;
   const T alpha = (T)a.ctrl->alpha, beta = (T)a.ctrl->beta;
   const T mu = (T)a.ctrl->mean[0], mv = (T)a.ctrl->mean[1], mw = (T)a.ctrl->mean[2];
-  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, k0 = blockIdx.z * KZ;
+  const int x0 = bx * TX, y0 = by * TY, k0 = bz * KZ;
   const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
   const int i = x0 + tx, j = y0 + ty;
   const size_t nn = (size_t)n * n;
@@ -206,6 +233,15 @@ __global__ void __launch_bounds__(NT) momentum_kernel(StencilArgs<T> a, int KZ) 
     if (m + 1 <= k0 + KZ) issue(m + 1);
     else cp_async_commit();
     cp_async_wait<1>();  // this thread's copies of plane m have landed
+    // rhs_o of the output plane k = m-1, loaded now so that its latency hides
+    // behind the force computation below
+    T ruo = 0, rvo = 0, rwo = 0;
+    if (m >= k0 + 1) {
+      const size_t g = (size_t)i + (size_t)n * j + nn * wrapi(m - 1, n);
+      ruo = a.ru[g];
+      rvo = a.rv[g];
+      rwo = a.rw[g];
+    }
     {
       // the pending mean removal, on the elements this thread copied
       const int sl = (m + 8) & 3;
@@ -306,7 +342,6 @@ __global__ void __launch_bounds__(NT) momentum_kernel(StencilArgs<T> a, int KZ) 
       }
       // B6, B7 (multi/main.f90:666-681)
       const size_t g = (size_t)i + (size_t)n * j + nn * kz;
-      const T ruo = a.ru[g], rvo = a.rv[g], rwo = a.rw[g];
       a.us[g] = uc + dt * (alpha * ru - beta * ruo);
       a.vs[g] = vc + dt * (alpha * rv - beta * rvo);
       a.ws[g] = wc + dt * (alpha * rw - beta * rwo);
@@ -323,17 +358,18 @@ __global__ void __launch_bounds__(NT) momentum_kernel(StencilArgs<T> a, int KZ) 
 constexpr int PKZ = 16;
 
 template <class T>
-__global__ void __launch_bounds__(NT, 4) project_kernel(StencilArgs<T> a) {
+__device__ __forceinline__ void project_body(const StencilArgs<T>& a, int bx, int by, int bz, int gx, int gy) {
   if (a.ctrl->status) return;
   const int n = a.c.n;
   const T dtr = (T)a.c.dtr, dxi = (T)a.c.dxi;
-  const int i = blockIdx.x * TX + threadIdx.x % TX, j = blockIdx.y * TY + threadIdx.x / TX;
-  const int k0 = blockIdx.z * PKZ;
+  const int i = bx * TX + threadIdx.x % TX, j = by * TY + threadIdx.x / TX;
+  const int k0 = bz * PKZ;
   const int im = i ? i - 1 : n - 1, jm = j ? j - 1 : n - 1;
   const size_t nn = (size_t)n * n;
   double su = 0, sv = 0, sw = 0;
   double xu = -INFINITY, xv = -INFINITY, xw = -INFINITY;
   T pprev = a.p[(size_t)i + (size_t)n * j + nn * wrapi(k0 - 1, n)];
+#pragma unroll 4
   for (int k = k0; k < k0 + PKZ; ++k) {
     const size_t g = (size_t)i + (size_t)n * j + nn * k;
     const T pc = a.p[g];
@@ -377,7 +413,7 @@ __global__ void __launch_bounds__(NT, 4) project_kernel(StencilArgs<T> a) {
       for (int t = 0; t < 3; ++t) r[t] += red[w][t];
       for (int t = 3; t < 6; ++t) r[t] = fmax(r[t], red[w][t]);
     }
-    const size_t b = (size_t)blockIdx.x + (size_t)gridDim.x * (blockIdx.y + (size_t)gridDim.y * blockIdx.z);
+    const size_t b = (size_t)bx + (size_t)gx * (by + (size_t)gy * bz);
     for (int t = 0; t < 6; ++t) a.partials[b * 6 + t] = r[t];
   }
 }
@@ -388,12 +424,13 @@ __global__ void __launch_bounds__(NT, 4) project_kernel(StencilArgs<T> a) {
 // u = ustar - dt/rho*(p - p_m)*dxi is evaluated in FP64 and rounded to FP32
 // only when stored, and the forward-difference divergence of the FP64
 // projected field is reduced (max |div u|) before that rounding.
-__global__ void __launch_bounds__(NT) project_refine_kernel(StencilArgs<float> a, const float* __restrict__ dp) {
+__device__ __forceinline__ void project_refine_body(const StencilArgs<float>& a, const float* __restrict__ dp, int bx,
+                                                    int by, int bz, int gx, int gy) {
   if (a.ctrl->status) return;
   const int n = a.c.n;
   const double dtr = a.c.dtr, dxi = a.c.dxi;
-  const int i = blockIdx.x * TX + threadIdx.x % TX, j = blockIdx.y * TY + threadIdx.x / TX;
-  const int k0 = blockIdx.z * PKZ;
+  const int i = bx * TX + threadIdx.x % TX, j = by * TY + threadIdx.x / TX;
+  const int k0 = bz * PKZ;
   const int im = i ? i - 1 : n - 1, jm = j ? j - 1 : n - 1;
   const int ip = (i + 1 == n) ? 0 : i + 1, jp = (j + 1 == n) ? 0 : j + 1;
   const size_t nn = (size_t)n * n;
@@ -456,7 +493,7 @@ __global__ void __launch_bounds__(NT) project_refine_kernel(StencilArgs<float> a
       for (int t = 0; t < 3; ++t) r[t] += red[w][t];
       for (int t = 3; t < 7; ++t) r[t] = fmax(r[t], red[w][t]);
     }
-    const size_t b = (size_t)blockIdx.x + (size_t)gridDim.x * (blockIdx.y + (size_t)gridDim.y * blockIdx.z);
+    const size_t b = (size_t)bx + (size_t)gx * (by + (size_t)gy * bz);
     for (int t = 0; t < 7; ++t) a.partials[b * 7 + t] = r[t];
   }
 }
@@ -471,8 +508,8 @@ constexpr int FNT = 1024;
 
 // Partials hold `stride` values per CTA: sums of u, v, w, maxima of u, v, w,
 // and (stride 7, FP32 refine form) the max |div u| of the FP64 projection.
-__global__ void __launch_bounds__(FNT) finalize_kernel(const double* __restrict__ partials, int nparts, int stride,
-                                                       Ctrl* ctrl, StepConst c) {
+__device__ __forceinline__ void finalize_body(const double* __restrict__ partials, int nparts, int stride, Ctrl* ctrl,
+                                              const StepConst& c) {
   if (ctrl->status) return;
   double v[7] = {0, 0, 0, -INFINITY, -INFINITY, -INFINITY, 0};
   for (int b = threadIdx.x; b < nparts; b += FNT) {
@@ -520,6 +557,69 @@ __global__ void __launch_bounds__(FNT) finalize_kernel(const double* __restrict_
   }
 }
 
+// ============================================================ entry points
+// Single simulation: block coordinates are the grid's.
+template <class T>
+__global__ void __launch_bounds__(PNT, 2) phase_kernel(StencilArgs<T> a, int KZ) {
+  phase_body<T>(a, KZ, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+template <class T, bool PF, int MTYv>
+__global__ void __launch_bounds__(TX * MTYv, 32 / MTYv) momentum_kernel(StencilArgs<T> a, int KZ) {
+  momentum_body<T, PF, MTYv>(a, KZ, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+template <class T>
+__global__ void __launch_bounds__(NT, 4) project_kernel(StencilArgs<T> a) {
+  project_body<T>(a, blockIdx.x, blockIdx.y, blockIdx.z, gridDim.x, gridDim.y);
+}
+__global__ void __launch_bounds__(NT) project_refine_kernel(StencilArgs<float> a, const float* __restrict__ dp) {
+  project_refine_body(a, dp, blockIdx.x, blockIdx.y, blockIdx.z, gridDim.x, gridDim.y);
+}
+__global__ void __launch_bounds__(FNT) finalize_kernel(const double* __restrict__ partials, int nparts, int stride,
+                                                       Ctrl* ctrl, StepConst c) {
+  finalize_body(partials, nparts, stride, ctrl, c);
+}
+
+// Batched over the slots of a served ensemble: grid z (x for finalize)
+// covers the slots; each slot runs exactly the arithmetic of a single
+// simulation, so a result is the same alone and in any mix.
+template <class T>
+__global__ void __launch_bounds__(PNT, 2) phase_kernel_b(const SlotArgs<T>* __restrict__ slots, int KZ, int zch) {
+  const int sl = blockIdx.z / zch;
+  if (!slots[sl].active) return;
+  StencilArgs<T> a = slots[sl].st;
+  const int par = (int)(a.ctrl->nstep & 1);
+  a.phi_in = slots[sl].phi[par];
+  a.phi_out = slots[sl].phi[par ^ 1];
+  phase_body<T>(a, KZ, blockIdx.x, blockIdx.y, blockIdx.z - sl * zch);
+}
+template <class T, bool PF, int MTYv>
+__global__ void __launch_bounds__(TX * MTYv, 32 / MTYv) momentum_kernel_b(const SlotArgs<T>* __restrict__ slots, int KZ,
+                                                                         int zch) {
+  const int sl = blockIdx.z / zch;
+  if (!slots[sl].active) return;
+  StencilArgs<T> a = slots[sl].st;
+  if (PF) a.phi_in = slots[sl].phi[(int)((a.ctrl->nstep + 1) & 1)];  // the updated phi
+  momentum_body<T, PF, MTYv>(a, KZ, blockIdx.x, blockIdx.y, blockIdx.z - sl * zch);
+}
+template <class T>
+__global__ void __launch_bounds__(NT, 4) project_kernel_b(const SlotArgs<T>* __restrict__ slots, int zch) {
+  const int sl = blockIdx.z / zch;
+  if (!slots[sl].active) return;
+  project_body<T>(slots[sl].st, blockIdx.x, blockIdx.y, blockIdx.z - sl * zch, gridDim.x, gridDim.y);
+}
+__global__ void __launch_bounds__(NT) project_refine_kernel_b(const SlotArgs<float>* __restrict__ slots, int zch) {
+  const int sl = blockIdx.z / zch;
+  if (!slots[sl].active) return;
+  project_refine_body(slots[sl].st, slots[sl].dp, blockIdx.x, blockIdx.y, blockIdx.z - sl * zch, gridDim.x,
+                      gridDim.y);
+}
+template <class T>
+__global__ void __launch_bounds__(FNT) finalize_kernel_b(const SlotArgs<T>* __restrict__ slots, int nparts, int stride) {
+  const int sl = blockIdx.x;
+  if (!slots[sl].active) return;
+  finalize_body(slots[sl].st.partials, nparts, stride, slots[sl].st.ctrl, slots[sl].st.c);
+}
+
 // u -= mean in place, then mean = 0 (materialises the lazy mean removal).
 template <class T>
 __global__ void materialize_kernel(T* u, T* v, T* w, size_t count, Ctrl* ctrl) {
@@ -541,9 +641,9 @@ __global__ void clear_mean_kernel(Ctrl* ctrl) {
 template <class T> static size_t phase_smem() {
   return sizeof(T) * (size_t)(8 * (TX + 4) * (PTY + 4) + 9 * (TX + 2) * (PTY + 2));
 }
-template <class T> static size_t momentum_smem(bool pf) {
-  size_t s = 3 * 4 * (TX + 2) * (TY + 2);
-  if (pf) s += 4 * (TX + 4) * (TY + 4) + 2 * 3 * (TX + 1) * (TY + 1);
+template <class T> static size_t momentum_smem(bool pf, int mty) {
+  size_t s = 3 * 4 * (TX + 2) * (mty + 2);
+  if (pf) s += 4 * (TX + 4) * (mty + 4) + 2 * 3 * (TX + 1) * (mty + 1);
   return sizeof(T) * s;
 }
 
@@ -557,11 +657,17 @@ template <class T> static cudaError_t prep_t() {
   cudaError_t e;
   if ((e = cudaFuncSetAttribute(phase_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)phase_smem<T>())))
     return e;
-  if ((e = cudaFuncSetAttribute(momentum_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)momentum_smem<T>(true))))
-    return e;
-  if ((e = cudaFuncSetAttribute(momentum_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)momentum_smem<T>(false))))
+  const void* mk[8] = {(const void*)momentum_kernel<T, true, 8>, (const void*)momentum_kernel<T, false, 8>,
+                       (const void*)momentum_kernel<T, true, 16>, (const void*)momentum_kernel<T, false, 16>,
+                       (const void*)momentum_kernel_b<T, true, 8>, (const void*)momentum_kernel_b<T, false, 8>,
+                       (const void*)momentum_kernel_b<T, true, 16>, (const void*)momentum_kernel_b<T, false, 16>};
+  for (int q = 0; q < 8; ++q) {
+    const bool pf = (q % 2) == 0;
+    const int mty = ((q / 2) % 2) ? 16 : 8;
+    if ((e = cudaFuncSetAttribute(mk[q], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)momentum_smem<T>(pf, mty))))
+      return e;
+  }
+  if ((e = cudaFuncSetAttribute(phase_kernel_b<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)phase_smem<T>())))
     return e;
   return cudaSuccess;
 }
@@ -572,20 +678,27 @@ cudaError_t prepare_stencils() {
   return prep_t<float>();
 }
 
-template <class T> cudaError_t launch_phase(const StencilArgs<T>& a, cudaStream_t st) {
-  const int n = a.c.n, kz = pick_kz(n);
+template <class T> cudaError_t launch_phase(const StencilArgs<T>& a, cudaStream_t st, int kz) {
+  const int n = a.c.n;
+  if (kz <= 0) kz = pick_kz(n);
   dim3 grid(n / TX, n / PTY, n / kz);
   phase_kernel<T><<<grid, PNT, phase_smem<T>(), st>>>(a, kz);
   return cudaGetLastError();
 }
 
-template <class T> cudaError_t launch_momentum(const StencilArgs<T>& a, bool pf, cudaStream_t st) {
-  const int n = a.c.n, kz = pick_kz(n);
-  dim3 grid(n / TX, n / TY, n / kz);
-  if (pf)
-    momentum_kernel<T, true><<<grid, NT, momentum_smem<T>(true), st>>>(a, kz);
-  else
-    momentum_kernel<T, false><<<grid, NT, momentum_smem<T>(false), st>>>(a, kz);
+template <class T> cudaError_t launch_momentum(const StencilArgs<T>& a, bool pf, cudaStream_t st, int kz, int mty) {
+  const int n = a.c.n;
+  if (kz <= 0) kz = pick_kz(n);
+  if (mty != 8) mty = 16;
+  dim3 grid(n / TX, n / mty, n / kz);
+  const size_t sm = momentum_smem<T>(pf, mty);
+  if (mty == 8) {
+    if (pf) momentum_kernel<T, true, 8><<<grid, TX * 8, sm, st>>>(a, kz);
+    else momentum_kernel<T, false, 8><<<grid, TX * 8, sm, st>>>(a, kz);
+  } else {
+    if (pf) momentum_kernel<T, true, 16><<<grid, TX * 16, sm, st>>>(a, kz);
+    else momentum_kernel<T, false, 16><<<grid, TX * 16, sm, st>>>(a, kz);
+  }
   return cudaGetLastError();
 }
 
@@ -618,10 +731,57 @@ template <class T> cudaError_t launch_materialize(T* u, T* v, T* w, int n, Ctrl*
   return cudaGetLastError();
 }
 
-template cudaError_t launch_phase<double>(const StencilArgs<double>&, cudaStream_t);
-template cudaError_t launch_phase<float>(const StencilArgs<float>&, cudaStream_t);
-template cudaError_t launch_momentum<double>(const StencilArgs<double>&, bool, cudaStream_t);
-template cudaError_t launch_momentum<float>(const StencilArgs<float>&, bool, cudaStream_t);
+int stencil_kz_ok(int n, int kz) { return kz >= 2 && kz <= n && n % kz == 0; }
+
+template <class T>
+cudaError_t launch_phase_batched(const SlotArgs<T>* slots, int nslots, int n, int kz, cudaStream_t st) {
+  dim3 grid(n / TX, n / PTY, (n / kz) * nslots);
+  phase_kernel_b<T><<<grid, PNT, phase_smem<T>(), st>>>(slots, kz, n / kz);
+  return cudaGetLastError();
+}
+template <class T>
+cudaError_t launch_momentum_batched(const SlotArgs<T>* slots, int nslots, int n, int kz, bool pf, cudaStream_t st,
+                                   int mty) {
+  if (mty != 8) mty = 16;
+  dim3 grid(n / TX, n / mty, (n / kz) * nslots);
+  const size_t sm = momentum_smem<T>(pf, mty);
+  if (mty == 8) {
+    if (pf) momentum_kernel_b<T, true, 8><<<grid, TX * 8, sm, st>>>(slots, kz, n / kz);
+    else momentum_kernel_b<T, false, 8><<<grid, TX * 8, sm, st>>>(slots, kz, n / kz);
+  } else {
+    if (pf) momentum_kernel_b<T, true, 16><<<grid, TX * 16, sm, st>>>(slots, kz, n / kz);
+    else momentum_kernel_b<T, false, 16><<<grid, TX * 16, sm, st>>>(slots, kz, n / kz);
+  }
+  return cudaGetLastError();
+}
+template <class T>
+cudaError_t launch_project_batched(const SlotArgs<T>* slots, int nslots, int n, cudaStream_t st) {
+  dim3 grid(n / TX, n / TY, (n / PKZ) * nslots);
+  if constexpr (sizeof(T) == 8)
+    project_kernel_b<T><<<grid, NT, 0, st>>>(slots, n / PKZ);
+  else
+    project_refine_kernel_b<<<grid, NT, 0, st>>>(slots, n / PKZ);
+  return cudaGetLastError();
+}
+template cudaError_t launch_project_batched<double>(const SlotArgs<double>*, int, int, cudaStream_t);
+template cudaError_t launch_project_batched<float>(const SlotArgs<float>*, int, int, cudaStream_t);
+cudaError_t launch_finalize_batched(const SlotArgs<double>* slots, int nslots, int n, cudaStream_t st) {
+  finalize_kernel_b<double><<<nslots, FNT, 0, st>>>(slots, project_partials(n), 6);
+  return cudaGetLastError();
+}
+cudaError_t launch_finalize_batched_f32(const SlotArgs<float>* slots, int nslots, int n, cudaStream_t st) {
+  finalize_kernel_b<float><<<nslots, FNT, 0, st>>>(slots, project_partials(n), 7);
+  return cudaGetLastError();
+}
+template cudaError_t launch_phase_batched<double>(const SlotArgs<double>*, int, int, int, cudaStream_t);
+template cudaError_t launch_phase_batched<float>(const SlotArgs<float>*, int, int, int, cudaStream_t);
+template cudaError_t launch_momentum_batched<double>(const SlotArgs<double>*, int, int, int, bool, cudaStream_t, int);
+template cudaError_t launch_momentum_batched<float>(const SlotArgs<float>*, int, int, int, bool, cudaStream_t, int);
+
+template cudaError_t launch_phase<double>(const StencilArgs<double>&, cudaStream_t, int);
+template cudaError_t launch_phase<float>(const StencilArgs<float>&, cudaStream_t, int);
+template cudaError_t launch_momentum<double>(const StencilArgs<double>&, bool, cudaStream_t, int, int);
+template cudaError_t launch_momentum<float>(const StencilArgs<float>&, bool, cudaStream_t, int, int);
 template cudaError_t launch_project<double>(const StencilArgs<double>&, cudaStream_t);
 template cudaError_t launch_project<float>(const StencilArgs<float>&, cudaStream_t);
 template cudaError_t launch_materialize<double>(double*, double*, double*, int, Ctrl*, cudaStream_t);

@@ -145,6 +145,17 @@ class Solver:
         self._check(self.lib.mhit_diagnostics(self.h, int(pi_f32), ctypes.byref(st)), "mhit_diagnostics")
         return st.as_dict()
 
+    def drops(self):
+        """Drop count and sizes of the current phi (post/DropCountSize convention):
+        returns (cells, deq), numpy arrays in the reference's discovery order."""
+        nd = ctypes.c_int()
+        self._check(self.lib.mhit_drop_count(self.h, 0, ctypes.byref(nd), None, None), "mhit_drop_count")
+        cells = np.empty(max(nd.value, 1), dtype=np.int64)
+        deq = np.empty(max(nd.value, 1))
+        self._check(self.lib.mhit_drop_count(self.h, nd.value, ctypes.byref(nd), cells.ctypes.data, deq.ctypes.data),
+                    "mhit_drop_count")
+        return cells[:nd.value], deq[:nd.value]
+
     # -- files
     def save(self, outdir: str, t: int):
         os.makedirs(outdir, exist_ok=True)
@@ -192,6 +203,10 @@ class Solver:
         for k in range(ns.value):
             out[self.lib.mhit_stage_name(self.h, k).decode()] = ms[k]
         return out
+
+    def set_tiles(self, kz: int = 0, mty: int = 0):
+        """Stencil z chunk and momentum tile height (0 = defaults); results do not depend on them."""
+        self._check(self.lib.mhit_set_tiles(self.h, kz, mty), "mhit_set_tiles")
 
     def stream(self) -> int:
         return self.lib.mhit_stream(self.h)

@@ -10,4 +10,4 @@ reference legs may import this package, and only as the checker / the timed
 CPU stand-in for the reference.  The product library (``mhit36_b200``) never
 imports, links or calls it.
 """
-from .oracle import Oracle, OracleParams, build_oracle, dissipation, fft1d, lib_path  # noqa: F401
+from .oracle import Oracle, OracleParams, build_oracle, dissipation, drop_count, fft1d, lib_path  # noqa: F401

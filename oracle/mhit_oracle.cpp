@@ -691,4 +691,48 @@ double oracle_dissipation(int n, const double* u, const double* v, const double*
   return 2 * nu * eps / n / n / n;
 }
 
+// Drop count and sizes, post/DropCountSize: cells with phi >= 0.5
+// (get_interface.f90:15), the x-fastest scan starting a new drop at every
+// foreground cell not yet taken (get_interface.f90:28-40), the flood fill over
+// the 26 neighbours with periodic wrap (flood_fill.f90:1-127; iterative here,
+// the recursion overflows the stack for large drops), and
+// deq = dx*(6/pi*vol)^(1/3) (calculate_deq.f90:29-33).  Returns the count;
+// the first `capacity` drops' cell counts and diameters go to cells / deq.
+int oracle_drop_count(int n, const double* phi, int capacity, int64_t* cells, double* deq, double dx) {
+  const size_t N3 = (size_t)n * n * n, nn = (size_t)n * n;
+  std::vector<unsigned char> top(N3);
+  for (size_t g = 0; g < N3; ++g) top[g] = phi[g] >= 0.5 ? 1 : 0;
+  const double pi = 4.0 * std::atan(1.0), n6opi = 6.0 / pi;
+  int count = 0;
+  std::vector<size_t> stack;
+  for (size_t g0 = 0; g0 < N3; ++g0) {
+    if (!top[g0]) continue;
+    ++count;
+    int64_t vol = 0;
+    top[g0] = 0;
+    stack.assign(1, g0);
+    while (!stack.empty()) {
+      const size_t g = stack.back();
+      stack.pop_back();
+      ++vol;
+      const int i = (int)(g % n), j = (int)((g / n) % n), k = (int)(g / nn);
+      for (int dk = -1; dk <= 1; ++dk)
+        for (int dj = -1; dj <= 1; ++dj)
+          for (int di = -1; di <= 1; ++di) {
+            if (!di && !dj && !dk) continue;
+            const size_t nb = (size_t)((i + di + n) % n) + (size_t)n * ((j + dj + n) % n) + nn * ((k + dk + n) % n);
+            if (top[nb]) {
+              top[nb] = 0;
+              stack.push_back(nb);
+            }
+          }
+    }
+    if (count <= capacity) {
+      cells[count - 1] = vol;
+      deq[count - 1] = dx * std::pow(n6opi * (double)vol, 1.0 / 3.0);
+    }
+  }
+  return count;
+}
+
 }  // extern "C"

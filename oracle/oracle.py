@@ -82,6 +82,8 @@ def _load():
         lib.oracle_fft1d.argtypes = [ctypes.c_int, dp, ctypes.c_int]
         lib.oracle_dissipation.argtypes = [ctypes.c_int, dp, dp, dp, ctypes.c_double, ctypes.c_int]
         lib.oracle_dissipation.restype = ctypes.c_double
+        lib.oracle_drop_count.argtypes = [ctypes.c_int, dp, ctypes.c_int, ctypes.c_void_p, dp, ctypes.c_double]
+        lib.oracle_drop_count.restype = ctypes.c_int
         _lib = lib
     return _lib
 
@@ -183,3 +185,15 @@ def dissipation(u, v, w, nu: float, pi_f32: bool = True) -> float:
     n = u.shape[0]
     a = [_raw(x, n) for x in (u, v, w)]
     return lib.oracle_dissipation(n, *[_ptr(x) for x in a], nu, 1 if pi_f32 else 0)
+
+
+def drop_count(phi, dx: float):
+    """post/DropCountSize on a raw field indexed [i,j,k]: (cells, deq) in discovery order."""
+    lib = _load()
+    n = phi.shape[0]
+    a = _raw(phi, n)
+    cap = 1 << 16
+    cells = np.empty(cap, dtype=np.int64)
+    deq = np.empty(cap)
+    cnt = lib.oracle_drop_count(n, _ptr(a), cap, cells.ctypes.data, _ptr(deq), dx)
+    return cells[:min(cnt, cap)], deq[:min(cnt, cap)]

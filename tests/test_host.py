@@ -166,3 +166,22 @@ def test_create_without_gpu_fails_cleanly():
     from mhit36_b200 import Solver, MhitError
     with pytest.raises(MhitError):
         Solver(32, phase_field=False)
+
+
+def test_vtk_export_format(tmp_path):
+    from mhit36_b200 import vtk
+    n = 8
+    rng = np.random.default_rng(3)
+    u = rng.standard_normal((n, n, n))
+    phi = rng.random((n, n, n))
+    path = vtk.write_vtk(vtk.vtk_name(str(tmp_path), 42), {"u": u, "phi": phi})
+    assert path.endswith("OUTPAR_00000042.vtk")
+    raw = open(path, "rb").read()
+    assert raw.startswith(b"# vtk DataFile Version 3.0\nPhase field\nBINARY\nDATASET RECTILINEAR_GRID\n")
+    assert b"DIMENSIONS        8       8       8\n" in raw  # Fortran i8 fields
+    assert b"POINT_DATA              512\n" in raw          # i16
+    back = vtk.read_vtk(path)
+    assert back["dims"] == [n, n, n]
+    assert np.array_equal(back["u"], u.astype(np.float32))
+    assert np.array_equal(back["phi"], phi.astype(np.float32))
+    assert abs(float(back["coords"][0][-1]) - 2 * np.pi) < 1e-6  # x(n) = 2 pi on the reference grid

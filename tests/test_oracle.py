@@ -99,3 +99,17 @@ def test_oracle_cfl_stop(oracle_mod):
     o.set_fields(u, v, w)
     rc, d = o.step(3, cfl_limit=1e-6)
     assert rc == 1 and d["step"] == 1
+
+
+def test_oracle_drop_count_rules(oracle_mod):
+    """post/DropCountSize rules: threshold 0.5, 26-connectivity, periodic wrap, scan order."""
+    n = 16
+    phi = np.zeros((n, n, n))
+    phi[2:5, 2:5, 2:5] = 1.0              # 27 cells, first in scan order
+    phi[10, 10, 10] = phi[11, 11, 11] = 1  # corner contact only: one drop (26-connected)
+    phi[15, 7, 7] = phi[0, 7, 7] = 0.5     # across the x boundary, exactly at the threshold
+    phi[7, 0, 3] = 0.4999                  # below the threshold
+    dx = 2 * np.pi / (n - 1)
+    cells, deq = oracle_mod.drop_count(phi, dx)
+    assert list(cells) == [27, 2, 2]
+    assert np.allclose(deq, dx * (6 / np.pi * cells) ** (1 / 3), rtol=0, atol=1e-15)
