@@ -38,25 +38,38 @@ if ROOT not in sys.path:
 
 METRIC = "Mpts*steps/s at 512^3 NS+ACDI (FP64 plain form)"
 UNIT = "Mpts*steps/s"
-# Compulsory HBM traffic per grid point per step, FP64 NS+ACDI: 35 field passes
-# (each stage reads its inputs once and writes its outputs once).
-ALGO_BYTES_STEP = {"fp64": {True: 280, False: 232}}
+# Compulsory HBM traffic per grid point per step under a schedule in which
+# each stage reads its inputs once and writes its outputs once, the half
+# spectrum counts as one field pass and the inverse x transform feeds the
+# projection without storing p: FP64 NS+ACDI 35 field passes (280 B), NS-only
+# 29 (232 B).  The FP32 refinement form: 50 four-byte passes with ACDI
+# (200 B), 44 without (176 B) -- the same passes plus the residual and the
+# second solve.
+ALGO_BYTES_STEP = {"fp64": {True: 280, False: 232}, "fp32": {True: 200, False: 176}}
 
 
-def kernel_bytes_per_point(n: int, pf: bool) -> dict:
-    """Algorithmic HBM bytes per grid point for each kernel (FP64)."""
-    spec = 16.0 * (n // 2 + 1) / n  # half spectrum, complex128
-    return {
-        "phase": 40.0,                     # read u,v,w,phi; write phi
-        "momentum": 104.0 if pf else 96.0,  # read u,v,w,rhs_o(3)[,phi]; write ustar(3), rhs_o(3)
-        "xfwd": 24.0 + spec,               # read ustar(3); write half spectrum
+def kernel_bytes_per_point(n: int, pf: bool, precision: str = "fp64") -> dict:
+    """Algorithmic HBM bytes per grid point for each kernel of the form."""
+    e = 8.0 if precision == "fp64" else 4.0   # bytes per stored real
+    spec = 2 * e * (n // 2 + 1) / n           # half spectrum, complex
+    kb = {
+        "phase": 5 * e,                           # read u,v,w,phi; write phi
+        "momentum": (13 if pf else 12) * e,       # read u,v,w,rhs_o(3)[,phi]; write ustar(3), rhs_o(3)
+        "xfwd": 3 * e + spec,                     # read ustar(3); write half spectrum
         "yfwd": 2 * spec,
         "zsolve": 2 * spec,
         "yinv": 2 * spec,
-        "xinv": spec + 8.0,                # read spectrum; write p
-        "project": 56.0,                   # read p, ustar(3); write u,v,w
+        "xinv": spec + e,                         # read spectrum; write p (p0)
+        "project": 7 * e,                         # read p, ustar(3); write u,v,w
         "finalize": 0.0,
     }
+    if precision != "fp64":
+        # second solve, of the FP64 residual r - L(p0): read ustar(3) and p0,
+        # write the half spectrum; the same column passes; write dp.  The
+        # projection also reads dp.
+        kb.update({"xres": 4 * e + spec, "yfwd2": 2 * spec, "zsolve2": 2 * spec, "yinv2": 2 * spec,
+                   "xinv2": spec + e, "project": 8 * e})
+    return kb
 
 
 def parse():
@@ -78,10 +91,13 @@ def parse():
     return ap.parse_args()
 
 
-def workload(n, pf, dt):
+def workload(n, pf, dt, precision="fp64"):
     from mhit36_b200 import fields
     from mhit36_b200.config import InputParams
-    p = InputParams(dt=dt, mu=6e-3, rho=1.0, sigma=0.5, epsr=1.0, lin_force=0.1)
+    # the FP32 refinement form solves with the FD-modified k^2 (the symbol of
+    # the 7-point Laplacian its FP64 residual uses)
+    p = InputParams(dt=dt, mu=6e-3, rho=1.0, sigma=0.5, epsr=1.0, lin_force=0.1,
+                    k2_mode=1 if precision == "fp32" else 0)
     if n >= 512:
         recipe = (64, 0.2, 0.35)
     else:
@@ -229,7 +245,7 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
     pf = not args.ns_only
     n = args.n
-    p, case, recipe = workload(n, pf, args.dt)
+    p, case, recipe = workload(n, pf, args.dt, args.precision)
     s = Solver(n, p, precision=args.precision, phase_field=pf)
     s.set_fields(*case)
     stream = torch.cuda.ExternalStream(s.stream())
@@ -265,20 +281,20 @@ def main():
 
     # per-kernel durations (individually launched, CUDA events on the stream)
     prof = s.profile_step(3)
-    kb = kernel_bytes_per_point(n, pf)
+    kb = kernel_bytes_per_point(n, pf, args.precision)
     dominant = max(prof, key=lambda k: prof[k])
     peak, peak_kind = peaks()
     npts = n ** 3
     dom_bytes = kb[dominant] * npts
     achieved = dom_bytes / (prof[dominant] / 1e3) / 1e9
     step_ms = ms / args.steps
-    step_bytes = ALGO_BYTES_STEP["fp64"][pf] * npts
+    step_bytes = ALGO_BYTES_STEP[args.precision][pf] * npts
     roofline = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
                 "algo_bytes_per_launch": dom_bytes,
                 "per_kernel_ms": {k: round(v, 4) for k, v in prof.items()},
                 "per_kernel_gbs": {k: round(kb[k] * npts / (v / 1e3) / 1e9, 1) for k, v in prof.items() if kb[k]},
-                "step": {"algo_bytes_per_point": ALGO_BYTES_STEP["fp64"][pf],
+                "step": {"algo_bytes_per_point": ALGO_BYTES_STEP[args.precision][pf],
                          "achieved": step_bytes / (step_ms / 1e3) / 1e9,
                          "frac": step_bytes / (step_ms / 1e3) / 1e9 / peak}}
 

@@ -469,7 +469,7 @@ int mhit_create(const mhit_params* p, int nx, int ny, int nz, int precision, int
     if ((e = mhit::prepare_poisson(n))) { fail(e, "prepare_poisson"); break; }
     if ((e = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking))) { fail(e, "stream"); break; }
     const size_t N3 = (size_t)n * n * n;
-    const size_t pitch = mhit::spectrum_pitch(n);
+    const size_t pitch = mhit::spectrum_pitch(n, precision != MHIT_FP64);
     bool bad = false;
     if (precision == MHIT_FP64) {
       const size_t fb = N3 * sizeof(double);

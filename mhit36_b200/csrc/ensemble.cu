@@ -134,7 +134,7 @@ size_t elem(int precision) { return precision == MHIT_FP64 ? sizeof(double) : si
 size_t slot_bytes(int n, int pf, int precision) {
   const size_t N3 = (size_t)n * n * n, e = elem(precision);
   size_t fields = 9 + 1 + (pf ? 2 : 0) + (precision == MHIT_FP64 ? 0 : 1);  // + p / (p0, dp)
-  const size_t spec = (size_t)n * n * mhit::spectrum_pitch(n) * 2 * e;
+  const size_t spec = (size_t)n * n * mhit::spectrum_pitch(n, precision != MHIT_FP64) * 2 * e;
   return fields * N3 * e + spec + (size_t)mhit::project_partials(n) * 7 * sizeof(double) + 2 * n * sizeof(double);
 }
 
@@ -341,7 +341,7 @@ cudaError_t alloc_slot_buffers(mhit_ensemble* e, Class* c, SlotBuf& b) {
   }
   for (int q = 9; q < nf; ++q)
     if ((r = get(N3 * el, &b.f[11 + (q - 9)]))) return r;
-  const size_t spec = (size_t)n * n * mhit::spectrum_pitch(n) * 2 * el;
+  const size_t spec = (size_t)n * n * mhit::spectrum_pitch(n, c->precision != MHIT_FP64) * 2 * el;
   if ((r = get(spec, &b.f[13]))) return r;
   if ((r = cudaMemsetAsync(b.f[13], 0, spec, c->st))) return r;
   if ((r = get((size_t)mhit::project_partials(n) * 7 * sizeof(double), &b.f[14]))) return r;

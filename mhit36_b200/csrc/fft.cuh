@@ -96,8 +96,16 @@ template <class C> __device__ __forceinline__ C ldg_c(const C* p) { return __ldg
 // One Stockham stage over L interleaved lines, NT threads.
 template <int L> struct Pitch { static constexpr int value = L + 1; };
 
-template <int N, int R, int NS, int L, int NT, int DIR, class C>
-__device__ __forceinline__ void fft_stage(C* s, const C* __restrict__ tw) {
+// Identity post-processing of a stage's outputs.
+struct NoPost {
+  template <class C> __device__ __forceinline__ C operator()(int, int, C v) const { return v; }
+};
+
+// `post(k, l, v)` is applied to every output of the stage (k: index along the
+// line, l: line) before it is stored; the last stage of a transform uses it
+// to fuse a per-mode scaling.
+template <int N, int R, int NS, int L, int NT, int DIR, class C, class Post = NoPost>
+__device__ __forceinline__ void fft_stage(C* s, const C* __restrict__ tw, const Post& post = Post()) {
   constexpr int LP = Pitch<L>::value;
   constexpr int NR = N / R;
   constexpr int W = L * NR;
@@ -131,18 +139,23 @@ __device__ __forceinline__ void fft_stage(C* s, const C* __restrict__ tw) {
       const int jm = j % NS;
       const int d0 = (j / NS) * NS * R + jm;
 #pragma unroll
-      for (int r = 0; r < R; ++r) s[(d0 + r * NS) * LP + l] = v[it][r];
+      for (int r = 0; r < R; ++r) s[(d0 + r * NS) * LP + l] = post(d0 + r * NS, l, v[it][r]);
     }
   }
   __syncthreads();
 }
 
 template <int N, int NS, int L, int NT, int DIR, class C> struct FFTRun {
-  static __device__ __forceinline__ void run(C* s, const C* __restrict__ tw) {
+  template <class Post>
+  static __device__ __forceinline__ void run(C* s, const C* __restrict__ tw, const Post& post) {
     if constexpr (NS < N) {
       constexpr int R = pick_radix(N / NS);
-      fft_stage<N, R, NS, L, NT, DIR, C>(s, tw);
-      FFTRun<N, NS * R, L, NT, DIR, C>::run(s, tw);
+      if constexpr (NS * R == N) {
+        fft_stage<N, R, NS, L, NT, DIR, C, Post>(s, tw, post);
+      } else {
+        fft_stage<N, R, NS, L, NT, DIR, C>(s, tw);
+        FFTRun<N, NS * R, L, NT, DIR, C>::run(s, tw, post);
+      }
     }
   }
 };
@@ -151,7 +164,14 @@ template <int N, int NS, int L, int NT, int DIR, class C> struct FFTRun {
 // Must be called by all NT threads of the CTA; ends with a barrier.
 template <int N, int L, int NT, int DIR, class C>
 __device__ __forceinline__ void smem_fft(C* s, const C* __restrict__ tw) {
-  FFTRun<N, 1, L, NT, DIR, C>::run(s, tw);
+  FFTRun<N, 1, L, NT, DIR, C>::run(s, tw, NoPost());
+}
+
+// The same, with post(k, l, v) applied to every output (mode k of line l)
+// as the last stage stores it.
+template <int N, int L, int NT, int DIR, class C, class Post>
+__device__ __forceinline__ void smem_fft_post(C* s, const C* __restrict__ tw, const Post& post) {
+  FFTRun<N, 1, L, NT, DIR, C>::run(s, tw, post);
 }
 
 }  // namespace mhit

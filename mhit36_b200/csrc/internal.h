@@ -28,7 +28,8 @@ template <class T> cudaError_t launch_poisson(int n, const PoissonArgs<T>& a, cu
 // One of the five Poisson kernels (0 xfwd, 1 yfwd, 2 zsolve, 3 yinv, 4 xinv).
 template <class T> cudaError_t launch_poisson_stage(int n, const PoissonArgs<T>& a, int stage, cudaStream_t st);
 cudaError_t prepare_poisson(int n);
-size_t spectrum_pitch(int n);
+// Row pitch (complex elements) of the half spectrum of the FP64 (fp32 = 0) or FP32 form.
+size_t spectrum_pitch(int n, int fp32);
 
 template <class T> struct StencilArgs {
   const T* u;

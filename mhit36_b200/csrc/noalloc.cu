@@ -81,7 +81,7 @@ extern "C" int mhit_poisson_noalloc(const double* rhs_dev, double* p_dev, int n,
   Addrs a;
   int rc = setup_device(dev, &a);
   if (rc) return rc;
-  if (mhit::spectrum_pitch(n) > kPitchMax) return MHIT_ERR_SCRATCH_LIMIT;
+  if (mhit::spectrum_pitch(n, 0) > kPitchMax) return MHIT_ERR_SCRATCH_LIMIT;
   if (mhit::prepare_poisson(n) != cudaSuccess) return MHIT_ERR_CUDA;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
 

@@ -9,7 +9,7 @@
 //     The reference transforms the full complex field (2x the work).
 //   * Spectrum layout in HBM: spec[kz][ky][kx], kx fastest, row pitch PITCH
 //     complex (N/2+1 rounded up to the column chunk CC), so a chunk of CC
-//     kx columns is one 128-byte row segment.  The y and z passes stage a
+//     kx columns is one 32-128-byte row segment.  The y and z passes stage a
 //     CC x N slab in shared memory, transform along the slow axis there, and
 //     write it back in place: no transposes in HBM at all (the reference does
 //     four cuDecomp transposes per solve, multi/main.f90:754-810).
@@ -23,11 +23,14 @@
 
 namespace mhit {
 
-template <int N> struct PCfg {
-  // Lines per CTA: 2048/N (at most 8), so that the first radix-8 stage gives
-  // every one of the 256 threads exactly one butterfly (registers stay under
-  // the 85 that three resident CTAs per SM allow).
-  static constexpr int L = (N <= 256) ? 8 : ((N <= 512) ? 4 : 2);
+template <int N, class T = double> struct PCfg {
+  // Lines per CTA.  FP64: 2048/N (at most 8), so that the first radix-8 stage
+  // gives every one of the 256 threads exactly one butterfly (registers stay
+  // under the 85 that three resident CTAs per SM allow).  FP32: twice that
+  // (two butterflies per thread), so that a chunk of kx columns is still a
+  // 64-128-byte row segment of the half spectrum.
+  static constexpr int L = (sizeof(T) == 8) ? ((N <= 256) ? 8 : ((N <= 512) ? 4 : 2))
+                                            : ((N <= 256) ? 16 : ((N <= 512) ? 8 : 4));
   static constexpr int P = L;   // line pairs per CTA (x passes)
   static constexpr int CC = L;  // kx columns per CTA (y/z passes)
   static constexpr int NT = 256;
@@ -72,7 +75,7 @@ __device__ __forceinline__ void xfwd_body(const T* __restrict__ us, const T* __r
                                           const typename C2<T>::t* __restrict__ tw, const Ctrl* __restrict__ ctrl,
                                           double cdiv, double ddxi, int bx, int by) {
   typedef typename C2<T>::t C;
-  typedef PCfg<N> G;
+  typedef PCfg<N, T> G;
   constexpr int P = G::P, NT = G::NT;
   if (ctrl && ctrl->status) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -115,7 +118,7 @@ __device__ __forceinline__ void ypass_body(typename C2<T>::t* __restrict__ spec,
                                            const typename C2<T>::t* __restrict__ tw, const Ctrl* __restrict__ ctrl,
                                            int bx, int by) {
   typedef typename C2<T>::t C;
-  typedef PCfg<N> G;
+  typedef PCfg<N, T> G;
   constexpr int CC = G::CC, NT = G::NT;
   if (ctrl && ctrl->status) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -144,7 +147,7 @@ __device__ __forceinline__ void zsolve_body(typename C2<T>::t* __restrict__ spec
                                             const double* __restrict__ k2tab, const Ctrl* __restrict__ ctrl, int bx,
                                             int by) {
   typedef typename C2<T>::t C;
-  typedef PCfg<N> G;
+  typedef PCfg<N, T> G;
   constexpr int CC = G::CC, NT = G::NT;
   if (ctrl && ctrl->status) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -204,7 +207,7 @@ struct ColSlab {
 template <int N, int KIND, class T>
 __device__ __forceinline__ void colpass_issue(typename C2<T>::t* buf, const ColSlab& sl) {
   typedef typename C2<T>::t C;
-  typedef PCfg<N> G;
+  typedef PCfg<N, T> G;
   constexpr int CC = G::CC, NT = G::NT, LP = Pitch<CC>::value;
   if (sl.live) {
     const C* base = static_cast<const C*>(sl.spec);
@@ -219,7 +222,7 @@ __device__ __forceinline__ void colpass_issue(typename C2<T>::t* buf, const ColS
 template <int N, int KIND, class T>
 __device__ __forceinline__ void colpass_compute(typename C2<T>::t* s, const ColSlab& sl) {
   typedef typename C2<T>::t C;
-  typedef PCfg<N> G;
+  typedef PCfg<N, T> G;
   constexpr int CC = G::CC, NT = G::NT, LP = Pitch<CC>::value;
   const C* tw = static_cast<const C*>(sl.tw);
   if (KIND == 0) {
@@ -227,26 +230,26 @@ __device__ __forceinline__ void colpass_compute(typename C2<T>::t* s, const ColS
   } else if (KIND == 1) {
     smem_fft<N, CC, NT, +1>(s, tw);
   } else {
-    smem_fft<N, CC, NT, -1>(s, tw);
+    // forward z FFT whose last stage stores -psi/k2/(nx*ny*nz)
+    // (multi/main.f90:792, one reciprocal per mode), mode (0,0,0) and the
+    // pitch padding beyond kx = N/2 set to 0; then the inverse z FFT
     const double nnn = (double)((long long)N * (long long)N * (long long)N);
-    const double k2y = sl.k2tab[sl.jy];
-    for (int wi = threadIdx.x; wi < CC * N; wi += NT) {
-      const int l = wi % CC, n = wi / CC;
-      const int m = sl.m0 + l;
-      C v = s[n * LP + l];
-      if (m > N / 2 || (m == 0 && sl.jy == 0 && n == 0)) {
+    const double* k2tab = sl.k2tab;
+    const double k2y = k2tab[sl.jy];
+    const int m0 = sl.m0, jy = sl.jy;
+    smem_fft_post<N, CC, NT, -1>(s, tw, [=](int n, int l, C v) {
+      const int m = m0 + l;
+      if (m > N / 2 || (m == 0 && jy == 0 && n == 0)) {
         v.x = 0;
         v.y = 0;
       } else {
-        // -psi/k2/(nx*ny*nz) (multi/main.f90:792) as one reciprocal per mode
-        const double k2 = (sl.k2tab[m] + k2y) + sl.k2tab[n];
+        const double k2 = (k2tab[m] + k2y) + k2tab[n];
         const double f = -1.0 / (k2 * nnn);
         v.x = (T)((double)v.x * f);
         v.y = (T)((double)v.y * f);
       }
-      s[n * LP + l] = v;
-    }
-    __syncthreads();
+      return v;
+    });
     smem_fft<N, CC, NT, +1>(s, tw);
   }
   C* base = static_cast<C*>(sl.spec);
@@ -260,7 +263,7 @@ __device__ __forceinline__ void colpass_compute(typename C2<T>::t* s, const ColS
 template <int N, int KIND, class T>
 __device__ __forceinline__ ColSlab slab_single(typename C2<T>::t* spec, const void* tw, const double* k2tab,
                                                const Ctrl* ctrl, int it) {
-  typedef PCfg<N> G;
+  typedef PCfg<N, T> G;
   ColSlab sl;
   const int chunk = it % G::NCHUNK, line = it / G::NCHUNK;
   sl.live = !(ctrl && ctrl->status);
@@ -282,7 +285,7 @@ __device__ __forceinline__ ColSlab slab_single(typename C2<T>::t* spec, const vo
 template <int N, int KIND, class T, class Getter>
 __device__ __forceinline__ void colpass_run(int total, Getter get) {
   typedef typename C2<T>::t C;
-  typedef PCfg<N> G;
+  typedef PCfg<N, T> G;
   constexpr int LP = Pitch<G::CC>::value;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* buf0 = reinterpret_cast<C*>(smem_raw);
@@ -310,14 +313,14 @@ template <int N, int KIND, class T>
 __global__ void __launch_bounds__(256, 2) colpass_kernel(typename C2<T>::t* __restrict__ spec,
                                                      const typename C2<T>::t* __restrict__ tw,
                                                      const double* __restrict__ k2tab, const Ctrl* __restrict__ ctrl) {
-  typedef PCfg<N> G;
+  typedef PCfg<N, T> G;
   colpass_run<N, KIND, T>(G::NCHUNK * N, [&](int it) { return slab_single<N, KIND, T>(spec, tw, k2tab, ctrl, it); });
 }
 
 template <int N, int KIND, class T>
 __global__ void __launch_bounds__(256, 2) colpass_kernel_b(const SlotArgs<T>* __restrict__ slots, int nslots,
                                                        int which) {
-  typedef PCfg<N> G;
+  typedef PCfg<N, T> G;
   const int per = G::NCHUNK * N;
   colpass_run<N, KIND, T>(per * nslots, [&](int it) {
     const int sl = it / per;
@@ -340,7 +343,7 @@ __device__ __forceinline__ void xinv_body(const typename C2<T>::t* __restrict__ 
                                           const typename C2<T>::t* __restrict__ tw, const Ctrl* __restrict__ ctrl,
                                           int bx, int by) {
   typedef typename C2<T>::t C;
-  typedef PCfg<N> G;
+  typedef PCfg<N, T> G;
   constexpr int P = G::P, NT = G::NT;
   if (ctrl && ctrl->status) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -443,14 +446,14 @@ __global__ void __launch_bounds__(256, 3) xinv_kernel_b(const SlotArgs<T>* __res
 
 // ---------------------------------------------------------------- launchers
 template <int N, class T> static size_t xsmem() {
-  return (size_t)N * Pitch<PCfg<N>::P>::value * sizeof(typename C2<T>::t);
+  return (size_t)N * Pitch<PCfg<N, T>::P>::value * sizeof(typename C2<T>::t);
 }
 template <int N, class T> static size_t csmem() {
-  return (size_t)N * Pitch<PCfg<N>::CC>::value * sizeof(typename C2<T>::t);
+  return (size_t)N * Pitch<PCfg<N, T>::CC>::value * sizeof(typename C2<T>::t);
 }
 
 template <int N, class T> static size_t colsmem() {
-  return 2 * (size_t)N * Pitch<PCfg<N>::CC>::value * sizeof(typename C2<T>::t);
+  return 2 * (size_t)N * Pitch<PCfg<N, T>::CC>::value * sizeof(typename C2<T>::t);
 }
 
 // Persistent grid: resident CTAs per SM (occupancy) times the SM count.
@@ -497,7 +500,7 @@ template <int N, class T> static cudaError_t set_attrs() {
 
 template <int N, class T>
 static void launch_xfwd(const PoissonArgs<T>& a, cudaStream_t st) {
-  typedef PCfg<N> G;
+  typedef PCfg<N, T> G;
   const dim3 gx(N / (2 * G::P), N);
   const size_t xs = xsmem<N, T>();
   if (a.rhs)
@@ -513,7 +516,7 @@ static void launch_xfwd(const PoissonArgs<T>& a, cudaStream_t st) {
 
 template <int N, class T>
 static cudaError_t poisson_run(const PoissonArgs<T>& a, cudaStream_t st) {
-  typedef PCfg<N> G;
+  typedef PCfg<N, T> G;
   const dim3 gx(N / (2 * G::P), N), gc(G::NCHUNK, N);
   const size_t xs = xsmem<N, T>(), cs = csmem<N, T>();
   (void)gc;
@@ -529,7 +532,7 @@ static cudaError_t poisson_run(const PoissonArgs<T>& a, cudaStream_t st) {
 
 template <int N, class T>
 static cudaError_t poisson_stage(const PoissonArgs<T>& a, int stage, cudaStream_t st) {
-  typedef PCfg<N> G;
+  typedef PCfg<N, T> G;
   const dim3 gx(N / (2 * G::P), N), gc(G::NCHUNK, N);
   const size_t xs = xsmem<N, T>(), cs = csmem<N, T>();
   switch (stage) {
@@ -569,7 +572,7 @@ template cudaError_t launch_poisson_stage<float>(int, const PoissonArgs<float>&,
 
 template <int N, class T>
 static cudaError_t poisson_stage_b(const SlotArgs<T>* slots, int nslots, int stage, int which, cudaStream_t st) {
-  typedef PCfg<N> G;
+  typedef PCfg<N, T> G;
   const dim3 gx(N / (2 * G::P), N * nslots), gc(G::NCHUNK, N * nslots);
   const size_t xs = xsmem<N, T>(), cs = csmem<N, T>();
   switch (stage) {
@@ -634,11 +637,11 @@ cudaError_t launch_poisson(int n, const PoissonArgs<T>& a, cudaStream_t st) {
   }
 }
 
-size_t spectrum_pitch(int n) {
+size_t spectrum_pitch(int n, int fp32) {
   switch (n) {
 #define MHIT_CASE(NN) \
   case NN:            \
-    return PCfg<NN>::PITCH;
+    return fp32 ? PCfg<NN, float>::PITCH : PCfg<NN, double>::PITCH;
     MHIT_FOR_SIZES(MHIT_CASE)
 #undef MHIT_CASE
     default:

@@ -41,6 +41,21 @@ int default_mty(int n) { return n > 0 ? 8 : 8; }
 constexpr int PTY = 16;            // phase tile height
 constexpr int PNT = TX * PTY;       // phase threads per CTA
 
+// Momentum ring depth (planes per field) for a tile height.
+__host__ __device__ constexpr int momentum_ring(int mty) { return mty == 8 ? 5 : 4; }
+
+// 1/(sqrt(s) + tiny) for s > 0, the normalisation of A5.  With r = rsqrt(s),
+// 1/(sqrt(s) + tiny) = r/(1 + tiny*r) = r - tiny*r^2 + r*O((tiny*r)^2); the
+// first-order form is used while tiny*r < 2^-30, where the dropped term is
+// below 2^-60 r (far under an ulp), and the direct formula otherwise.
+template <class T>
+__device__ __forceinline__ T inv_norm_plus(T s, T tiny) {
+  const T r = rsqrt(s);
+  const T tr = tiny * r;
+  if (tr < (T)9.3e-10) return fma(-tr, r, r);
+  return (T)1 / (sqrt(s) + tiny);
+}
+
 template <class T>
 __device__ __forceinline__ void phase_body(const StencilArgs<T>& a, int KZ, int bx, int by, int bz) {
   if (a.ctrl->status) return;
@@ -68,58 +83,81 @@ __device__ __forceinline__ void phase_body(const StencilArgs<T>& a, int KZ, int 
   const int i = x0 + tx, j = y0 + ty;
   const int ip = (i + 1 == n) ? 0 : i + 1, jp = (j + 1 == n) ? 0 : j + 1;
   const size_t nn = (size_t)n * n;
+  // Each thread owns ring elements tid + r*NT of every plane (copy and psi)
+  // and F elements tid + r*NT; their in-plane offsets are the same on every
+  // plane, so they are computed once here.
+  constexpr int NPE = (PE + NT - 1) / NT, NFE = (FE + NT - 1) / NT;
+  int poff[NPE], fpe[NFE];
+#pragma unroll
+  for (int r = 0; r < NPE; ++r) {
+    const int e = min(tid + r * NT, PE - 1);
+    poff[r] = wrapi(x0 - 2 + e % EX, n) + n * wrapi(y0 - 2 + e / EX, n);
+  }
+#pragma unroll
+  for (int r = 0; r < NFE; ++r) {
+    const int e = min(tid + r * NT, FE - 1);
+    fpe[r] = (e % FX + 1) + (e / FX + 1) * EX;
+  }
+  // Ring slots by role, rotated once per plane (no per-plane index
+  // arithmetic): at iteration m the phi slots hold planes m-3 .. m+1 (m+1
+  // still in flight), the psi slots m-2 .. m (m being written), and the F
+  // slots m-3 .. m-1 (m-1 being written).
+  T *Phm3 = s_phi, *Phm2 = s_phi + PE, *Phm1 = s_phi + 2 * PE, *Ph0 = s_phi + 3 * PE, *Php1 = s_phi + 4 * PE;
+  T *PsW = s_psi, *Psm1 = s_psi + PE, *Psm2 = s_psi + 2 * PE;
+  T *FW = s_F, *Fm2 = s_F + 3 * FE, *Fm3 = s_F + 6 * FE;
+  const int gij = i + n * j, gipj = ip + n * j, gijp = i + n * jp;
 
-  // phi plane m (2-cell ring) is copied into ring slot (m+15)%5 with
-  // cp.async one iteration ahead of its use.
-  auto issue = [&](int m) {
-    T* Pphi = s_phi + ((m + 15) % 5) * PE;
+  // phi plane m (2-cell ring) is copied into `dst` with cp.async one
+  // iteration ahead of its use.
+  auto issue = [&](T* dst, int m) {
     const T* src = a.phi_in + (size_t)wrapi(m, n) * nn;
-    for (int e = tid; e < PE; e += NT) {
-      const int ex = e % EX, ey = e / EX;
-      cp_async_elem(Pphi + e, src + (size_t)wrapi(x0 - 2 + ex, n) + (size_t)n * wrapi(y0 - 2 + ey, n));
+#pragma unroll
+    for (int r = 0; r < NPE; ++r) {
+      const int e = tid + r * NT;
+      if (r < NPE - 1 || e < PE) cp_async_elem(dst + e, src + poff[r]);
     }
     cp_async_commit();
   };
-  issue(k0 - 2);
+  issue(Ph0, k0 - 2);
   for (int m = k0 - 2; m <= k0 + KZ + 1; ++m) {
     __syncthreads();  // every thread is done with the slots plane m+1 reuses
-    if (m + 1 <= k0 + KZ + 1) issue(m + 1);
+    if (m + 1 <= k0 + KZ + 1) issue(Php1, m + 1);
     else cp_async_commit();
     cp_async_wait<1>();  // this thread's copies of plane m have landed
     // velocities of the output plane k = m-2, loaded now so that their latency
     // hides behind the psi and F work below
     T uc = 0, uxp = 0, vc = 0, vyp = 0, wc = 0, wzp = 0;
     if (m >= k0 + 2) {
-      const int kz = wrapi(m - 2, n), kzp = wrapi(m - 1, n);
-      const size_t g = (size_t)i + (size_t)n * j + nn * kz;
-      uc = a.u[g];
-      uxp = a.u[(size_t)ip + (size_t)n * j + nn * kz];
-      vc = a.v[g];
-      vyp = a.v[(size_t)i + (size_t)n * jp + nn * kz];
-      wc = a.w[g];
-      wzp = a.w[(size_t)i + (size_t)n * j + nn * kzp];
+      const size_t zo = nn * wrapi(m - 2, n), zop = nn * wrapi(m - 1, n);
+      uc = a.u[zo + gij];
+      uxp = a.u[zo + gipj];
+      vc = a.v[zo + gij];
+      vyp = a.v[zo + gijp];
+      wc = a.w[zo + gij];
+      wzp = a.w[zop + gij];
     }
     // (1) psi of plane m on the elements this thread copied.
-    {
-      const T* Pphi = s_phi + ((m + 15) % 5) * PE;
-      T* Ppsi = s_psi + ((m + 15) % 3) * PE;
-      for (int e = tid; e < PE; e += NT) {
-        const T val = fmax(fmin(Pphi[e], (T)1), floor0);
-        Ppsi[e] = (val == (T)0) ? psi0 : ((val == (T)1) ? psi1 : eps * log((val + enumv) / ((T)1 - val + enumv)));
+#pragma unroll
+    for (int r = 0; r < NPE; ++r) {
+      const int e = tid + r * NT;
+      if (r < NPE - 1 || e < PE) {
+        const T val = fmax(fmin(Ph0[e], (T)1), floor0);
+        PsW[e] = (val == (T)0) ? psi0 : ((val == (T)1) ? psi1 : eps * log((val + enumv) / ((T)1 - val + enumv)));
       }
     }
     __syncthreads();
     // (2) F on plane m-1 over the tile + 1 ring.
     if (m >= k0) {
-      const int fm = m - 1;
-      const T* Pc = s_psi + ((fm + 15) % 3) * PE;
-      const T* Pm = s_psi + ((fm + 14) % 3) * PE;
-      const T* Pp = s_psi + ((fm + 16) % 3) * PE;
-      const T* Phc = s_phi + ((fm + 15) % 5) * PE;
-      T* F = s_F + ((fm + 15) % 3) * 3 * FE;
-      for (int e = tid; e < FE; e += NT) {
-        const int fx = e % FX, fy = e / FX;
-        const int pe = (fx + 1) + (fy + 1) * EX;
+      const T* Pc = Psm1;
+      const T* Pm = Psm2;
+      const T* Pp = PsW;
+      const T* Phc = Phm1;
+      T* F = FW;
+#pragma unroll
+      for (int r = 0; r < NFE; ++r) {
+        const int e = tid + r * NT;
+        if (r == NFE - 1 && e >= FE) break;
+        const int pe = fpe[r];
         const T gxv = Pc[pe + 1] - Pc[pe - 1];
         const T gyv = Pc[pe + EX] - Pc[pe - EX];
         const T gzv = Pp[pe] - Pm[pe];
@@ -129,7 +167,7 @@ __device__ __forceinline__ void phase_body(const StencilArgs<T>& a, int KZ, int 
           F[2 * FE + e] = (T)0;
           continue;
         }
-        const T normod = (T)1 / (sqrt(gxv * gxv + gyv * gyv + gzv * gzv) + tiny);
+        const T normod = inv_norm_plus(gxv * gxv + gyv * gyv + gzv * gzv, tiny);
         T t;
         if (use_ident) {
           // tanh(0.5*log(a/b)) = (a-b)/(a+b) with a = val+enum, b = 1-val+enum
@@ -147,19 +185,17 @@ __device__ __forceinline__ void phase_body(const StencilArgs<T>& a, int KZ, int 
     __syncthreads();
     // (3) output plane k = m-2.
     if (m >= k0 + 2) {
-      const int k = m - 2;
-      const int kz = wrapi(k, n);
-      const T* P0 = s_phi + ((k + 15) % 5) * PE;
-      const T* Pm1 = s_phi + ((k + 14) % 5) * PE;
-      const T* Pp1 = s_phi + ((k + 16) % 5) * PE;
-      const T* F0 = s_F + ((k + 15) % 3) * 3 * FE;
-      const T* Fm = s_F + ((k + 14) % 3) * 3 * FE;
-      const T* Fp = s_F + ((k + 16) % 3) * 3 * FE;
+      const T* P0 = Phm2;
+      const T* Pm1 = Phm3;
+      const T* Pp1 = Phm1;
+      const T* F0 = Fm2;
+      const T* Fm = Fm3;
+      const T* Fp = FW;
       const int pe = (tx + 2) + (ty + 2) * EX;
       const int fe = (tx + 1) + (ty + 1) * FX;
       const T c = P0[pe], pxp = P0[pe + 1], pxm = P0[pe - 1], pyp = P0[pe + EX], pym = P0[pe - EX];
       const T pzp = Pp1[pe], pzm = Pm1[pe];
-      const size_t g = (size_t)i + (size_t)n * j + nn * kz;
+      const size_t g = nn * wrapi(m - 2, n) + gij;
       uc -= mu; uxp -= mu; vc -= mv; vyp -= mv; wc -= mw; wzp -= mw;
       const T h = (T)0.5;
       T r = -(uxp * h * (pxp + c) - uc * h * (c + pxm)) * dxi - (vyp * h * (pyp + c) - vc * h * (c + pym)) * dxi -
@@ -170,6 +206,14 @@ __device__ __forceinline__ void phase_body(const StencilArgs<T>& a, int KZ, int 
                        (Fp[2 * FE + fe] - Fm[2 * FE + fe]) * h * dxi);
       a.phi_out[g] = c + dt * r;
     }
+    // rotate the rings for plane m+1: the slot of the oldest plane of each
+    // ring takes the next plane
+    T* t = Phm3;
+    Phm3 = Phm2; Phm2 = Phm1; Phm1 = Ph0; Ph0 = Php1; Php1 = t;
+    t = Psm2;
+    Psm2 = Psm1; Psm1 = PsW; PsW = t;
+    t = Fm3;
+    Fm3 = Fm2; Fm2 = FW; FW = t;
   }
 }
 
@@ -187,12 +231,16 @@ __device__ __forceinline__ void momentum_body(const StencilArgs<T>& a, int KZ, i
   constexpr int UX = TX + 2, UY = TY + 2, UE = UX * UY;  // velocity planes, 1-cell ring
   constexpr int EX = TX + 4, EY = TY + 4, PE = EX * EY;  // phi planes, 2-cell ring
   constexpr int QX = TX + 1, QY = TY + 1, QE = QX * QY;  // force over [-1,TX) x [-1,TY)
+  // Ring of NS planes per field: planes m-2 .. m+PD at iteration m, the
+  // last PD of them in flight (two planes of prefetch for 8-row tiles, whose
+  // deeper ring still lets three CTAs share an SM; one for 16-row tiles).
+  constexpr int NS = momentum_ring(MTYv), PD = NS - 3;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* s_u = reinterpret_cast<T*>(smem_raw);  // ring of 4 planes each
-  T* s_v = s_u + 4 * UE;
-  T* s_w = s_v + 4 * UE;
-  T* s_phi = s_w + 4 * UE;     // ring of 4 (PF only)
-  T* s_f = s_phi + 4 * PE;     // ring of 2 planes x 3 components (PF only)
+  T* s_u = reinterpret_cast<T*>(smem_raw);
+  T* s_v = s_u + NS * UE;
+  T* s_w = s_v + NS * UE;
+  T* s_phi = s_w + NS * UE;    // PF only
+  T* s_f = s_phi + NS * PE;    // ring of 2 planes x 3 components (PF only)
   const int n = a.c.n;
   const T dxi = (T)a.c.dxi, ddxi = (T)a.c.ddxi, dt = (T)a.c.dt, mu_v = (T)a.c.mu, rhoi = (T)a.c.rhoi;
   const T eps = (T)a.c.eps, epsi = (T)a.c.epsi, sig6 = (T)(6.0 * a.c.sigma), lin = (T)a.c.lin_force;
@@ -204,35 +252,65 @@ __device__ __forceinline__ void momentum_body(const StencilArgs<T>& a, int KZ, i
   const int i = x0 + tx, j = y0 + ty;
   const size_t nn = (size_t)n * n;
   const T h = (T)0.5, q = (T)0.25;
+  // Each thread owns elements tid + r*NT of the velocity, phi and force
+  // planes; their in-plane offsets are the same on every plane.
+  constexpr int NUE = (UE + NT - 1) / NT, NPE = (PE + NT - 1) / NT, NQE = (QE + NT - 1) / NT;
+  int uoff[NUE], poff[NPE], qpe[NQE];
+#pragma unroll
+  for (int r = 0; r < NUE; ++r) {
+    const int e = min(tid + r * NT, UE - 1);
+    uoff[r] = wrapi(x0 - 1 + e % UX, n) + n * wrapi(y0 - 1 + e / UX, n);
+  }
+#pragma unroll
+  for (int r = 0; r < NPE; ++r) {
+    const int e = min(tid + r * NT, PE - 1);
+    poff[r] = PF ? wrapi(x0 - 2 + e % EX, n) + n * wrapi(y0 - 2 + e / EX, n) : 0;
+  }
+#pragma unroll
+  for (int r = 0; r < NQE; ++r) {
+    const int e = min(tid + r * NT, QE - 1);
+    qpe[r] = (e % QX + 1) + (e / QX + 1) * EX;
+  }
+  // sl[q] is the ring slot of plane m-2+q at iteration m; the roles rotate
+  // once per plane.
+  int sl[NS];
+#pragma unroll
+  for (int q2 = 0; q2 < NS; ++q2) sl[q2] = q2;
 
-  // Plane m of u, v, w (1-cell ring) and phi (2-cell ring) is copied into
-  // ring slot (m+8)&3 with cp.async one iteration ahead of its use, so the
-  // HBM latency of plane m+1 overlaps the arithmetic of plane m-1.
-  auto issue = [&](int m) {
-    const int sl = (m + 8) & 3;
+  // Plane m of u, v, w (1-cell ring) and phi (2-cell ring) is copied into a
+  // ring slot with cp.async PD iterations ahead of its use, so the HBM
+  // latency of the planes in flight overlaps the arithmetic of plane m-1.
+  auto issue = [&](int slot, int m) {
     const size_t zoff = (size_t)wrapi(m, n) * nn;
-    for (int e = tid; e < UE; e += NT) {
-      const int ex = e % UX, ey = e / UX;
-      const size_t gg = zoff + (size_t)wrapi(x0 - 1 + ex, n) + (size_t)n * wrapi(y0 - 1 + ey, n);
-      cp_async_elem(s_u + sl * UE + e, a.u + gg);
-      cp_async_elem(s_v + sl * UE + e, a.v + gg);
-      cp_async_elem(s_w + sl * UE + e, a.w + gg);
+    const T* su = a.u + zoff;
+    const T* sv = a.v + zoff;
+    const T* sw = a.w + zoff;
+#pragma unroll
+    for (int r = 0; r < NUE; ++r) {
+      const int e = tid + r * NT;
+      if (r < NUE - 1 || e < UE) {
+        cp_async_elem(s_u + slot * UE + e, su + uoff[r]);
+        cp_async_elem(s_v + slot * UE + e, sv + uoff[r]);
+        cp_async_elem(s_w + slot * UE + e, sw + uoff[r]);
+      }
     }
     if (PF) {
-      for (int e = tid; e < PE; e += NT) {
-        const int ex = e % EX, ey = e / EX;
-        cp_async_elem(s_phi + sl * PE + e,
-                      a.phi_in + zoff + (size_t)wrapi(x0 - 2 + ex, n) + (size_t)n * wrapi(y0 - 2 + ey, n));
+      const T* sp = a.phi_in + zoff;
+#pragma unroll
+      for (int r = 0; r < NPE; ++r) {
+        const int e = tid + r * NT;
+        if (r < NPE - 1 || e < PE) cp_async_elem(s_phi + slot * PE + e, sp + poff[r]);
       }
     }
     cp_async_commit();
   };
-  issue(k0 - 2);
+#pragma unroll
+  for (int q2 = 0; q2 < PD; ++q2) issue(sl[2 + q2], k0 - 2 + q2);
   for (int m = k0 - 2; m <= k0 + KZ; ++m) {
-    __syncthreads();  // every thread is done with the slot plane m+1 reuses
-    if (m + 1 <= k0 + KZ) issue(m + 1);
+    __syncthreads();  // every thread is done with the slot plane m+PD reuses
+    if (m + PD <= k0 + KZ) issue(sl[NS - 1], m + PD);
     else cp_async_commit();
-    cp_async_wait<1>();  // this thread's copies of plane m have landed
+    cp_async_wait<PD>();  // this thread's copies of plane m have landed
     // rhs_o of the output plane k = m-1, loaded now so that its latency hides
     // behind the force computation below
     T ruo = 0, rvo = 0, rwo = 0;
@@ -244,24 +322,30 @@ __device__ __forceinline__ void momentum_body(const StencilArgs<T>& a, int KZ, i
     }
     {
       // the pending mean removal, on the elements this thread copied
-      const int sl = (m + 8) & 3;
-      for (int e = tid; e < UE; e += NT) {
-        s_u[sl * UE + e] -= mu;
-        s_v[sl * UE + e] -= mv;
-        s_w[sl * UE + e] -= mw;
+      const int s0 = sl[2];
+#pragma unroll
+      for (int r = 0; r < NUE; ++r) {
+        const int e = tid + r * NT;
+        if (r < NUE - 1 || e < UE) {
+          s_u[s0 * UE + e] -= mu;
+          s_v[s0 * UE + e] -= mv;
+          s_w[s0 * UE + e] -= mw;
+        }
       }
     }
     __syncthreads();
     if (PF && m >= k0) {
       // B4: chempot, grad(phi), f at plane m-1 (multi/main.f90:617-623)
       const int fm = m - 1;
-      const T* P0 = s_phi + ((fm + 8) & 3) * PE;
-      const T* Pm = s_phi + ((fm + 7) & 3) * PE;
-      const T* Pp = s_phi + ((fm + 9) & 3) * PE;
+      const T* P0 = s_phi + sl[1] * PE;
+      const T* Pm = s_phi + sl[0] * PE;
+      const T* Pp = s_phi + sl[2] * PE;
       T* F = s_f + ((fm + 8) & 1) * 3 * QE;
-      for (int e = tid; e < QE; e += NT) {
-        const int qx = e % QX, qy = e / QX;
-        const int pe = (qx + 1) + (qy + 1) * EX;
+#pragma unroll
+      for (int r = 0; r < NQE; ++r) {
+        const int e = tid + r * NT;
+        if (r == NQE - 1 && e >= QE) break;
+        const int pe = qpe[r];
         const T c = P0[pe], pxp = P0[pe + 1], pxm = P0[pe - 1], pyp = P0[pe + EX], pym = P0[pe - EX];
         const T pzp = Pp[pe], pzm = Pm[pe];
         const T chem = c * ((T)1 - c) * ((T)1 - (T)2 * c) * epsi -
@@ -275,15 +359,15 @@ __device__ __forceinline__ void momentum_body(const StencilArgs<T>& a, int KZ, i
     if (PF) __syncthreads();
     if (m >= k0 + 1) {
       const int k = m - 1;
-      const T* U0 = s_u + ((k + 8) & 3) * UE;
-      const T* Um = s_u + ((k + 7) & 3) * UE;
-      const T* Up = s_u + ((k + 9) & 3) * UE;
-      const T* V0 = s_v + ((k + 8) & 3) * UE;
-      const T* Vm = s_v + ((k + 7) & 3) * UE;
-      const T* Vp = s_v + ((k + 9) & 3) * UE;
-      const T* W0 = s_w + ((k + 8) & 3) * UE;
-      const T* Wm = s_w + ((k + 7) & 3) * UE;
-      const T* Wp = s_w + ((k + 9) & 3) * UE;
+      const T* U0 = s_u + sl[1] * UE;
+      const T* Um = s_u + sl[0] * UE;
+      const T* Up = s_u + sl[2] * UE;
+      const T* V0 = s_v + sl[1] * UE;
+      const T* Vm = s_v + sl[0] * UE;
+      const T* Vp = s_v + sl[2] * UE;
+      const T* W0 = s_w + sl[1] * UE;
+      const T* Wm = s_w + sl[0] * UE;
+      const T* Wp = s_w + sl[2] * UE;
       const int e = (tx + 1) + (ty + 1) * UX;
       const T uc = U0[e], uxp = U0[e + 1], uxm = U0[e - 1], uyp = U0[e + UX], uym = U0[e - UX];
       const T uzp = Up[e], uzm = Um[e], uxpym = U0[e + 1 - UX], uxpzm = Um[e + 1];
@@ -349,6 +433,11 @@ __device__ __forceinline__ void momentum_body(const StencilArgs<T>& a, int KZ, i
       a.rv[g] = rv;
       a.rw[g] = rw;
     }
+    // rotate: the slot of plane m-2 takes plane m+PD+1 at the next iteration
+    const int t = sl[0];
+#pragma unroll
+    for (int q2 = 0; q2 < NS - 1; ++q2) sl[q2] = sl[q2 + 1];
+    sl[NS - 1] = t;
   }
 }
 
@@ -368,14 +457,17 @@ __device__ __forceinline__ void project_body(const StencilArgs<T>& a, int bx, in
   const size_t nn = (size_t)n * n;
   double su = 0, sv = 0, sw = 0;
   double xu = -INFINITY, xv = -INFINITY, xw = -INFINITY;
-  T pprev = a.p[(size_t)i + (size_t)n * j + nn * wrapi(k0 - 1, n)];
-#pragma unroll 4
+  // read-only loads (ld.global.nc): the inputs never alias the outputs, so
+  // the unrolled iterations' loads can be in flight together
+  const T* p = a.p;
+  T pprev = __ldg(p + (size_t)i + (size_t)n * j + nn * wrapi(k0 - 1, n));
+#pragma unroll 2
   for (int k = k0; k < k0 + PKZ; ++k) {
     const size_t g = (size_t)i + (size_t)n * j + nn * k;
-    const T pc = a.p[g];
-    const T uo = a.us[g] - dtr * (pc - a.p[g - i + im]) * dxi;
-    const T vo = a.vs[g] - dtr * (pc - a.p[g + (size_t)n * jm - (size_t)n * j]) * dxi;
-    const T wo = a.ws[g] - dtr * (pc - pprev) * dxi;
+    const T pc = __ldg(p + g);
+    const T uo = __ldg(a.us + g) - dtr * (pc - __ldg(p + g - i + im)) * dxi;
+    const T vo = __ldg(a.vs + g) - dtr * (pc - __ldg(p + g + (size_t)n * jm - (size_t)n * j)) * dxi;
+    const T wo = __ldg(a.ws + g) - dtr * (pc - pprev) * dxi;
     pprev = pc;
     a.uo[g] = uo;
     a.vo[g] = vo;
@@ -435,26 +527,28 @@ __device__ __forceinline__ void project_refine_body(const StencilArgs<float>& a,
   const int ip = (i + 1 == n) ? 0 : i + 1, jp = (j + 1 == n) ? 0 : j + 1;
   const size_t nn = (size_t)n * n;
   const float* p0 = a.p;
-  auto P = [&](size_t g) { return (double)p0[g] + (double)dp[g]; };
+  // read-only loads (ld.global.nc): the inputs never alias the outputs
+  auto P = [&](size_t g) { return (double)__ldg(p0 + g) + (double)__ldg(dp + g); };
   double su = 0, sv = 0, sw = 0, mdiv = 0;
   double xu = -INFINITY, xv = -INFINITY, xw = -INFINITY;
   const size_t col = (size_t)i + (size_t)n * j;
   double pm = P(col + nn * wrapi(k0 - 1, n));
   double pc = P(col + nn * k0);
-  double wsc = (double)a.ws[col + nn * k0];
+  double wsc = (double)__ldg(a.ws + col + nn * k0);
+#pragma unroll 2
   for (int k = k0; k < k0 + PKZ; ++k) {
     const size_t g = col + nn * k;
     const int kp = (k + 1 == n) ? 0 : k + 1;
     const size_t gzp = col + nn * kp;
     const double pn = P(gzp);
-    const double wsn = (double)a.ws[gzp];
+    const double wsn = (double)__ldg(a.ws + gzp);
     const size_t gxm = g - i + im, gxp = g - i + ip;
     const size_t gym = g - (size_t)n * j + (size_t)n * jm, gyp = g - (size_t)n * j + (size_t)n * jp;
-    const double uo = (double)a.us[g] - dtr * (pc - P(gxm)) * dxi;
-    const double vo = (double)a.vs[g] - dtr * (pc - P(gym)) * dxi;
+    const double uo = (double)__ldg(a.us + g) - dtr * (pc - P(gxm)) * dxi;
+    const double vo = (double)__ldg(a.vs + g) - dtr * (pc - P(gym)) * dxi;
     const double wo = wsc - dtr * (pc - pm) * dxi;
-    const double u1 = (double)a.us[gxp] - dtr * (P(gxp) - pc) * dxi;
-    const double v1 = (double)a.vs[gyp] - dtr * (P(gyp) - pc) * dxi;
+    const double u1 = (double)__ldg(a.us + gxp) - dtr * (P(gxp) - pc) * dxi;
+    const double v1 = (double)__ldg(a.vs + gyp) - dtr * (P(gyp) - pc) * dxi;
     const double w1 = wsn - dtr * (pn - pc) * dxi;
     const double div = ((u1 - uo) + (v1 - vo) + (w1 - wo)) * dxi;
     mdiv = fmax(mdiv, fabs(div));
@@ -642,8 +736,9 @@ template <class T> static size_t phase_smem() {
   return sizeof(T) * (size_t)(8 * (TX + 4) * (PTY + 4) + 9 * (TX + 2) * (PTY + 2));
 }
 template <class T> static size_t momentum_smem(bool pf, int mty) {
-  size_t s = 3 * 4 * (TX + 2) * (mty + 2);
-  if (pf) s += 4 * (TX + 4) * (mty + 4) + 2 * 3 * (TX + 1) * (mty + 1);
+  const int ns = momentum_ring(mty);
+  size_t s = 3 * ns * (TX + 2) * (mty + 2);
+  if (pf) s += ns * (TX + 4) * (mty + 4) + 2 * 3 * (TX + 1) * (mty + 1);
   return sizeof(T) * s;
 }
 
