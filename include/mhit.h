@@ -288,13 +288,22 @@ typedef struct mhit_ens_stats_t {
   int32_t classes, slots;
 } mhit_ens_stats_t;
 
-/* hbm_budget_bytes = 0: 85% of the free device memory. */
+/* mhit_ens_submit flags */
+#define MHIT_ENS_KEEP_RESULT 1  /* keep the final fields for mhit_ens_result */
+#define MHIT_ENS_BORROW_INPUT 2 /* do not copy u, v, w, phi: the caller keeps them valid and unchanged
+                                   until the request is done, failed or cancelled */
+
+/* hbm_budget_bytes = 0: 85% of the free device memory.  Starts the
+ * ensemble's two transfer threads (host<->device copies of request fields). */
 int mhit_ens_create(size_t hbm_budget_bytes, int slots_per_class, mhit_ensemble** out);
-/* Queue a request (inputs are copied; raw layout float64). */
+/* Queue a request (raw layout float64 inputs, copied unless
+ * MHIT_ENS_BORROW_INPUT; flags = MHIT_ENS_* bits). */
 int mhit_ens_submit(mhit_ensemble* e, const mhit_params* p, int n, int precision, int phase_field, int nsteps,
-                    const double* u, const double* v, const double* w, const double* phi, int keep_result,
+                    const double* u, const double* v, const double* w, const double* phi, int flags,
                     int64_t* id);
-/* One scheduling round: complete, admit, advance every busy class one step. */
+/* One scheduling round; never waits on the device: publish finished
+ * requests, activate uploaded ones, admit what fits, and keep a few
+ * milliseconds of batched steps queued on every busy class. */
 int mhit_ens_progress(mhit_ensemble* e, int* pending);
 int mhit_ens_query(mhit_ensemble* e, int64_t id, mhit_ens_info* out);
 /* Final fields of a done request (keep_result = 1), raw layout float64. */

@@ -79,6 +79,7 @@ class MhitEnsStats(ctypes.Structure):
 
 
 RQ_QUEUED, RQ_RUNNING, RQ_DONE, RQ_FAILED, RQ_CANCELLED = range(5)
+MHIT_ENS_KEEP_RESULT, MHIT_ENS_BORROW_INPUT = 1, 2
 
 # Every symbol include/mhit.h declares (checked by the CPU tests).
 HEADER_SYMBOLS = [

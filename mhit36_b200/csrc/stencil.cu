@@ -41,8 +41,10 @@ int default_mty(int n) { return n > 0 ? 8 : 8; }
 constexpr int PTY = 16;            // phase tile height
 constexpr int PNT = TX * PTY;       // phase threads per CTA
 
-// Momentum ring depth (planes per field) for a tile height.
-__host__ __device__ constexpr int momentum_ring(int mty) { return mty == 8 ? 5 : 4; }
+// Momentum ring depth (planes per field): planes m-2 .. m+1, one in flight.
+// (A 5-plane ring with two planes in flight measured 30% slower on B200 at
+// 512^3: it leaves fewer CTAs per SM.)
+__host__ __device__ constexpr int momentum_ring(int) { return 4; }
 
 // 1/(sqrt(s) + tiny) for s > 0, the normalisation of A5.  With r = rsqrt(s),
 // 1/(sqrt(s) + tiny) = r/(1 + tiny*r) = r - tiny*r^2 + r*O((tiny*r)^2); the
@@ -232,8 +234,7 @@ __device__ __forceinline__ void momentum_body(const StencilArgs<T>& a, int KZ, i
   constexpr int EX = TX + 4, EY = TY + 4, PE = EX * EY;  // phi planes, 2-cell ring
   constexpr int QX = TX + 1, QY = TY + 1, QE = QX * QY;  // force over [-1,TX) x [-1,TY)
   // Ring of NS planes per field: planes m-2 .. m+PD at iteration m, the
-  // last PD of them in flight (two planes of prefetch for 8-row tiles, whose
-  // deeper ring still lets three CTAs share an SM; one for 16-row tiles).
+  // last PD of them in flight.
   constexpr int NS = momentum_ring(MTYv), PD = NS - 3;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* s_u = reinterpret_cast<T*>(smem_raw);
@@ -457,17 +458,14 @@ __device__ __forceinline__ void project_body(const StencilArgs<T>& a, int bx, in
   const size_t nn = (size_t)n * n;
   double su = 0, sv = 0, sw = 0;
   double xu = -INFINITY, xv = -INFINITY, xw = -INFINITY;
-  // read-only loads (ld.global.nc): the inputs never alias the outputs, so
-  // the unrolled iterations' loads can be in flight together
-  const T* p = a.p;
-  T pprev = __ldg(p + (size_t)i + (size_t)n * j + nn * wrapi(k0 - 1, n));
-#pragma unroll 2
+  T pprev = a.p[(size_t)i + (size_t)n * j + nn * wrapi(k0 - 1, n)];
+#pragma unroll 4
   for (int k = k0; k < k0 + PKZ; ++k) {
     const size_t g = (size_t)i + (size_t)n * j + nn * k;
-    const T pc = __ldg(p + g);
-    const T uo = __ldg(a.us + g) - dtr * (pc - __ldg(p + g - i + im)) * dxi;
-    const T vo = __ldg(a.vs + g) - dtr * (pc - __ldg(p + g + (size_t)n * jm - (size_t)n * j)) * dxi;
-    const T wo = __ldg(a.ws + g) - dtr * (pc - pprev) * dxi;
+    const T pc = a.p[g];
+    const T uo = a.us[g] - dtr * (pc - a.p[g - i + im]) * dxi;
+    const T vo = a.vs[g] - dtr * (pc - a.p[g + (size_t)n * jm - (size_t)n * j]) * dxi;
+    const T wo = a.ws[g] - dtr * (pc - pprev) * dxi;
     pprev = pc;
     a.uo[g] = uo;
     a.vo[g] = vo;
@@ -527,28 +525,26 @@ __device__ __forceinline__ void project_refine_body(const StencilArgs<float>& a,
   const int ip = (i + 1 == n) ? 0 : i + 1, jp = (j + 1 == n) ? 0 : j + 1;
   const size_t nn = (size_t)n * n;
   const float* p0 = a.p;
-  // read-only loads (ld.global.nc): the inputs never alias the outputs
-  auto P = [&](size_t g) { return (double)__ldg(p0 + g) + (double)__ldg(dp + g); };
+  auto P = [&](size_t g) { return (double)p0[g] + (double)dp[g]; };
   double su = 0, sv = 0, sw = 0, mdiv = 0;
   double xu = -INFINITY, xv = -INFINITY, xw = -INFINITY;
   const size_t col = (size_t)i + (size_t)n * j;
   double pm = P(col + nn * wrapi(k0 - 1, n));
   double pc = P(col + nn * k0);
-  double wsc = (double)__ldg(a.ws + col + nn * k0);
-#pragma unroll 2
+  double wsc = (double)a.ws[col + nn * k0];
   for (int k = k0; k < k0 + PKZ; ++k) {
     const size_t g = col + nn * k;
     const int kp = (k + 1 == n) ? 0 : k + 1;
     const size_t gzp = col + nn * kp;
     const double pn = P(gzp);
-    const double wsn = (double)__ldg(a.ws + gzp);
+    const double wsn = (double)a.ws[gzp];
     const size_t gxm = g - i + im, gxp = g - i + ip;
     const size_t gym = g - (size_t)n * j + (size_t)n * jm, gyp = g - (size_t)n * j + (size_t)n * jp;
-    const double uo = (double)__ldg(a.us + g) - dtr * (pc - P(gxm)) * dxi;
-    const double vo = (double)__ldg(a.vs + g) - dtr * (pc - P(gym)) * dxi;
+    const double uo = (double)a.us[g] - dtr * (pc - P(gxm)) * dxi;
+    const double vo = (double)a.vs[g] - dtr * (pc - P(gym)) * dxi;
     const double wo = wsc - dtr * (pc - pm) * dxi;
-    const double u1 = (double)__ldg(a.us + gxp) - dtr * (P(gxp) - pc) * dxi;
-    const double v1 = (double)__ldg(a.vs + gyp) - dtr * (P(gyp) - pc) * dxi;
+    const double u1 = (double)a.us[gxp] - dtr * (P(gxp) - pc) * dxi;
+    const double v1 = (double)a.vs[gyp] - dtr * (P(gyp) - pc) * dxi;
     const double w1 = wsn - dtr * (pn - pc) * dxi;
     const double div = ((u1 - uo) + (v1 - vo) + (w1 - wo)) * dxi;
     mdiv = fmax(mdiv, fabs(div));

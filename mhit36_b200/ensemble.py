@@ -30,6 +30,7 @@ class Ensemble:
             raise MhitError(rc, "mhit_ens_create")
         self.h = h
         self._n = {}
+        self._borrowed = {}  # borrowed input arrays, kept alive until release()
 
     def _check(self, rc, where):
         if rc:
@@ -53,15 +54,20 @@ class Ensemble:
         self.close()
 
     def submit(self, n: int, params: InputParams, u, v, w, phi=None, nsteps: int = 100, precision: str = "fp64",
-               keep: bool = True) -> int:
+               keep: bool = True, borrow: bool = False) -> int:
+        """Queue a request.  borrow=True hands the (raw-layout) input arrays to
+        the ensemble without a copy; they are held here until release()."""
         prec = {"fp64": capi.MHIT_FP64, "fp32": capi.MHIT_FP32_REFINE, "fp32_refine": capi.MHIT_FP32_REFINE}[precision]
         mp = make_params(params)
         arrs = [_to_raw(u, n), _to_raw(v, n), _to_raw(w, n), _to_raw(phi, n) if phi is not None else None]
         ptrs = [a.ctypes.data if a is not None else None for a in arrs]
+        flags = (capi.MHIT_ENS_KEEP_RESULT if keep else 0) | (capi.MHIT_ENS_BORROW_INPUT if borrow else 0)
         rid = ctypes.c_int64()
         self._check(self.lib.mhit_ens_submit(self.h, ctypes.byref(mp), n, prec, int(phi is not None), nsteps,
-                                             *ptrs, int(keep), ctypes.byref(rid)), "mhit_ens_submit")
+                                             *ptrs, flags, ctypes.byref(rid)), "mhit_ens_submit")
         self._n[rid.value] = (n, phi is not None)
+        if borrow:
+            self._borrowed[rid.value] = arrs
         return rid.value
 
     def progress(self) -> int:
@@ -88,6 +94,7 @@ class Ensemble:
 
     def release(self, rid: int):
         self._check(self.lib.mhit_ens_release(self.h, rid), "mhit_ens_release")
+        self._borrowed.pop(rid, None)
 
     def cancel(self, rid: int):
         self._check(self.lib.mhit_ens_cancel(self.h, rid), "mhit_ens_cancel")
