@@ -294,7 +294,7 @@ typedef struct mhit_ens_stats_t {
                                    until the request is done, failed or cancelled */
 
 /* hbm_budget_bytes = 0: 85% of the free device memory.  Starts the
- * ensemble's two transfer threads (host<->device copies of request fields). */
+ * ensemble's transfer threads (host<->device copies of request fields). */
 int mhit_ens_create(size_t hbm_budget_bytes, int slots_per_class, mhit_ensemble** out);
 /* Queue a request (raw layout float64 inputs, copied unless
  * MHIT_ENS_BORROW_INPUT; flags = MHIT_ENS_* bits). */

@@ -13,10 +13,11 @@
 //
 // Host side.  The scheduling round (mhit_ens_progress) never waits on the
 // device: it polls events, keeps a few milliseconds of rounds queued on every
-// busy class, and hands every host<->device transfer of request fields to two
-// transfer threads (uploads, downloads).  Each moves fields through two
-// pinned staging chunks (double-buffered, with the FP32 rounding done while
-// staging) on its own stream, so transfers overlap the rounds of every class.
+// busy class, and hands every host<->device transfer of request fields to
+// transfer threads (two for uploads, four for downloads).  Each moves fields
+// through two pinned staging chunks (double-buffered, with the FP32 rounding
+// done while staging) on its own stream, so transfers overlap the rounds of
+// every class.
 // Slot-table entries are written by one-thread kernels that take the entry
 // by value, in stream order with the class's rounds.
 //
@@ -288,7 +289,12 @@ struct mhit_ensemble {
   std::deque<int64_t> queue;
   std::vector<std::unique_ptr<Class>> classes;
   std::vector<cudaEvent_t> free_events;
-  Transfer xfer[2];  // [0] uploads, [1] downloads: neither waits behind the other
+  // Transfer threads: kUp for uploads, then kDown for downloads (a download
+  // ends in page-faulting copies into fresh host vectors, the slower side).
+  // Jobs go round-robin, so neither direction waits behind the other.
+  static constexpr int kUp = 2, kDown = 4;
+  Transfer xfer[kUp + kDown];
+  unsigned next_up = 0, next_down = 0;
   bool xfer_started = false;
   std::string last_error;
   long long rounds = 0, launches = 0;
@@ -733,7 +739,7 @@ int admit(mhit_ensemble* e, Request* r, int* err) {
   j.r = r;
   j.c = c;
   j.b = &b;
-  e->xfer[0].push(j);
+  e->xfer[e->next_up++ % mhit_ensemble::kUp].push(j);
   return 1;
 }
 
@@ -839,9 +845,10 @@ int mhit_ens_create(size_t hbm_budget_bytes, int slots_per_class, mhit_ensemble*
   e->budget = hbm_budget_bytes ? hbm_budget_bytes : (size_t)(0.85 * (double)freeb);
   e->slots_per_class = slots_per_class;
   e->t0 = now_s();
-  if (e->xfer[0].start(e->device) != cudaSuccess || e->xfer[1].start(e->device) != cudaSuccess) {
-    e->xfer[0].stop();
-    e->xfer[1].stop();
+  bool ok = true;
+  for (auto& x : e->xfer) ok = ok && x.start(e->device) == cudaSuccess;
+  if (!ok) {
+    for (auto& x : e->xfer) x.stop();
     cudaGetLastError();
     return MHIT_ERR_CUDA;
   }
@@ -915,7 +922,7 @@ int mhit_ens_progress(mhit_ensemble* e, int* pending) {
         j.r = r;
         j.c = c;
         j.b = &c->slots[r->slot];
-        e->xfer[1].push(j);
+        e->xfer[mhit_ensemble::kUp + e->next_down++ % mhit_ensemble::kDown].push(j);
       } else if (q != cudaErrorNotReady) {
         return fail(e, q, "cudaEventQuery(done_ev)");
       }
@@ -1130,10 +1137,8 @@ const char* mhit_ens_last_error(mhit_ensemble* e) { return e ? e->last_error.c_s
 
 int mhit_ens_destroy(mhit_ensemble* e) {
   if (!e) return MHIT_ERR_INVALID;
-  if (e->xfer_started) {  // finishes the queued jobs first
-    e->xfer[0].stop();
-    e->xfer[1].stop();
-  }
+  if (e->xfer_started)  // finishes the queued jobs first
+    for (auto& x : e->xfer) x.stop();
   for (auto& c : e->classes) cudaStreamSynchronize(c->st);
   for (auto& kv : e->reqs)
     if (kv.second->done_ev) cudaEventDestroy(kv.second->done_ev);

@@ -83,13 +83,8 @@ __device__ __forceinline__ void xfwd_body(const T* __restrict__ us, const T* __r
   constexpr int LP = Pitch<P>::value;
   const int j0 = bx * (2 * P);
   const int k = by;
-  // x-fastest: each warp reads 32 consecutive cells of the same lines; a
-  // fixed trip count (P*N is a multiple of NT) unrolled by 2 keeps two
-  // elements' loads in flight per thread
-  static_assert((P * N) % NT == 0, "x pass staging assumes whole rounds");
-#pragma unroll 2
-  for (int it = 0; it < P * N / NT; ++it) {
-    const int wi = threadIdx.x + it * NT;
+  // x-fastest: each warp reads 32 consecutive cells of the same lines
+  for (int wi = threadIdx.x; wi < P * N; wi += NT) {
     const int n = wi % N, p = wi / N;
     const int ja = j0 + 2 * p;
     C z;
@@ -357,27 +352,11 @@ __device__ __forceinline__ void xinv_body(const typename C2<T>::t* __restrict__ 
   constexpr int M = N / 2 + 1;
   const int j0 = bx * (2 * P);
   const int k = by;
-  // fixed trip count, fully unrolled: every load of the thread is issued
-  // before the first one is used
-  constexpr int ITERS = (P * M + NT - 1) / NT;
-  C Av[ITERS], Bv[ITERS];
-#pragma unroll
-  for (int it = 0; it < ITERS; ++it) {
-    const int wi = threadIdx.x + it * NT;
-    if (wi < P * M) {
-      const int m = wi % M, q = wi / M;
-      const C* row = spec + ((size_t)k * N + j0 + 2 * q) * G::PITCH;
-      Av[it] = row[m];
-      Bv[it] = row[G::PITCH + m];
-    }
-  }
-#pragma unroll
-  for (int it = 0; it < ITERS; ++it) {
-    const int wi = threadIdx.x + it * NT;
-    if (wi >= P * M) break;
+  for (int wi = threadIdx.x; wi < P * M; wi += NT) {
     const int m = wi % M, q = wi / M;
-    C A = Av[it];
-    C B = Bv[it];
+    const C* row = spec + ((size_t)k * N + j0 + 2 * q) * G::PITCH;
+    C A = row[m];
+    C B = row[G::PITCH + m];
     if (m == 0 || m == N / 2) {
       A.y = 0;
       B.y = 0;
