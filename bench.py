@@ -47,6 +47,15 @@ UNIT = "Mpts*steps/s"
 # second solve.
 ALGO_BYTES_STEP = {"fp64": {True: 280, False: 232}, "fp32": {True: 200, False: 176}}
 
+# DRAM bytes (read + write) per grid point per launch, from one ncu capture of
+# the FP64 kernels at 256^3 (dram__bytes_read.sum + dram__bytes_write.sum of
+# each launch / 256^3; the summary is profiles/kernels_fp64_256_full.md).  A
+# stencil or column pass touches every point the same way at any size, so
+# traffic scales with the points processed; a full 512^3 capture is too large
+# to take under ncu.
+DRAM_BYTES_PER_POINT_FP64 = {"momentum": 104.07, "phase": 40.23, "project": 54.11, "xfwd": 30.84,
+                             "yfwd": 13.49, "zsolve": 13.50, "yinv": 13.49, "xinv": 13.93}
+
 
 def kernel_bytes_per_point(n: int, pf: bool, precision: str = "fp64") -> dict:
     """Algorithmic HBM bytes per grid point for each kernel of the form."""
@@ -290,7 +299,10 @@ def main():
     step_ms = ms / args.steps
     step_bytes = ALGO_BYTES_STEP[args.precision][pf] * npts
     roofline = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                "frac": achieved / peak, "peak_kind": peak_kind,
+                "traffic": (DRAM_BYTES_PER_POINT_FP64[dominant] * npts
+                            if args.precision == "fp64" and pf and dominant in DRAM_BYTES_PER_POINT_FP64 else None),
+                "traffic_source": "ncu dram__bytes_read+write at 256^3, scaled by points",
                 "algo_bytes_per_launch": dom_bytes,
                 "per_kernel_ms": {k: round(v, 4) for k, v in prof.items()},
                 "per_kernel_gbs": {k: round(kb[k] * npts / (v / 1e3) / 1e9, 1) for k, v in prof.items() if kb[k]},
