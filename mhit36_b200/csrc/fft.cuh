@@ -91,8 +91,6 @@ template <int DIR, class C> struct DFT<3, DIR, C> {
   }
 };
 
-template <class C> __device__ __forceinline__ C ldg_c(const C* p) { return __ldg(p); }
-
 // One Stockham stage over L interleaved lines, NT threads.
 template <int L> struct Pitch { static constexpr int value = L + 1; };
 
@@ -122,7 +120,7 @@ __device__ __forceinline__ void fft_stage(C* s, const C* __restrict__ tw, const 
       for (int r = 0; r < R; ++r) {
         C a = s[(j + r * NR) * LP + l];
         if (NS > 1 && r > 0) {
-          C t = ldg_c(tw + r * jm * TSTRIDE);
+          C t = tw[r * jm * TSTRIDE];
           a = (DIR < 0) ? cmul(a, t) : cmulc(a, t);
         }
         v[it][r] = a;

@@ -220,11 +220,11 @@ __device__ __forceinline__ void colpass_issue(typename C2<T>::t* buf, const ColS
 }
 
 template <int N, int KIND, class T>
-__device__ __forceinline__ void colpass_compute(typename C2<T>::t* s, const ColSlab& sl) {
+__device__ __forceinline__ void colpass_compute(typename C2<T>::t* s, const ColSlab& sl,
+                                                const typename C2<T>::t* tw) {
   typedef typename C2<T>::t C;
   typedef PCfg<N, T> G;
   constexpr int CC = G::CC, NT = G::NT, LP = Pitch<CC>::value;
-  const C* tw = static_cast<const C*>(sl.tw);
   if (KIND == 0) {
     smem_fft<N, CC, NT, -1>(s, tw);
   } else if (KIND == 1) {
@@ -282,16 +282,20 @@ __device__ __forceinline__ ColSlab slab_single(typename C2<T>::t* spec, const vo
   return sl;
 }
 
+// `gtw`: the launch's twiddle table (every slab of a launch shares it), copied
+// once into shared memory after the two slab buffers.
 template <int N, int KIND, class T, class Getter>
-__device__ __forceinline__ void colpass_run(int total, Getter get) {
+__device__ __forceinline__ void colpass_run(int total, const typename C2<T>::t* __restrict__ gtw, Getter get) {
   typedef typename C2<T>::t C;
   typedef PCfg<N, T> G;
   constexpr int LP = Pitch<G::CC>::value;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* buf0 = reinterpret_cast<C*>(smem_raw);
   C* buf1 = buf0 + N * LP;
+  C* stw = buf1 + N * LP;
   int it = blockIdx.x;
   if (it >= total) return;
+  for (int q = threadIdx.x; q < N; q += G::NT) stw[q] = gtw[q];  // visible after the loop's first barrier
   ColSlab cur = get(it);
   colpass_issue<N, KIND, T>(buf0, cur);
   for (int t = 0; it < total; ++t) {
@@ -302,7 +306,7 @@ __device__ __forceinline__ void colpass_run(int total, Getter get) {
     colpass_issue<N, KIND, T>((t & 1) ? buf0 : buf1, next);
     cp_async_wait<1>();
     __syncthreads();
-    if (cur.live) colpass_compute<N, KIND, T>((t & 1) ? buf1 : buf0, cur);
+    if (cur.live) colpass_compute<N, KIND, T>((t & 1) ? buf1 : buf0, cur, stw);
     __syncthreads();
     it = nxt;
     cur = next;
@@ -314,7 +318,8 @@ __global__ void __launch_bounds__(256, 2) colpass_kernel(typename C2<T>::t* __re
                                                      const typename C2<T>::t* __restrict__ tw,
                                                      const double* __restrict__ k2tab, const Ctrl* __restrict__ ctrl) {
   typedef PCfg<N, T> G;
-  colpass_run<N, KIND, T>(G::NCHUNK * N, [&](int it) { return slab_single<N, KIND, T>(spec, tw, k2tab, ctrl, it); });
+  colpass_run<N, KIND, T>(G::NCHUNK * N, tw,
+                          [&](int it) { return slab_single<N, KIND, T>(spec, tw, k2tab, ctrl, it); });
 }
 
 template <int N, int KIND, class T>
@@ -322,7 +327,12 @@ __global__ void __launch_bounds__(256, 2) colpass_kernel_b(const SlotArgs<T>* __
                                                        int which) {
   typedef PCfg<N, T> G;
   const int per = G::NCHUNK * N;
-  colpass_run<N, KIND, T>(per * nslots, [&](int it) {
+  // the class's twiddle table, from any active slot (all share it)
+  const typename C2<T>::t* tw = nullptr;
+  for (int q = 0; q < nslots && !tw; ++q)
+    if (slots[q].active) tw = (which ? slots[q].pr : slots[q].po).tw;
+  if (!tw) return;
+  colpass_run<N, KIND, T>(per * nslots, tw, [&](int it) {
     const int sl = it / per;
     const PoissonArgs<T>& a = which ? slots[sl].pr : slots[sl].po;
     ColSlab s;
@@ -452,8 +462,8 @@ template <int N, class T> static size_t csmem() {
   return (size_t)N * Pitch<PCfg<N, T>::CC>::value * sizeof(typename C2<T>::t);
 }
 
-template <int N, class T> static size_t colsmem() {
-  return 2 * (size_t)N * Pitch<PCfg<N, T>::CC>::value * sizeof(typename C2<T>::t);
+template <int N, class T> static size_t colsmem() {  // two slab buffers + the twiddle table
+  return (2 * (size_t)N * Pitch<PCfg<N, T>::CC>::value + N) * sizeof(typename C2<T>::t);
 }
 
 // Persistent grid: resident CTAs per SM (occupancy) times the SM count.
