@@ -112,82 +112,6 @@ __device__ __forceinline__ void xfwd_body(const T* __restrict__ us, const T* __r
   }
 }
 
-// ---------------------------------------------------------------- y pass
-template <int N, int DIR, class T>
-__device__ __forceinline__ void ypass_body(typename C2<T>::t* __restrict__ spec,
-                                           const typename C2<T>::t* __restrict__ tw, const Ctrl* __restrict__ ctrl,
-                                           int bx, int by) {
-  typedef typename C2<T>::t C;
-  typedef PCfg<N, T> G;
-  constexpr int CC = G::CC, NT = G::NT;
-  if (ctrl && ctrl->status) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* s = reinterpret_cast<C*>(smem_raw);
-  C* base = spec + (size_t)by * N * G::PITCH + bx * CC;
-  constexpr int LP = Pitch<CC>::value;
-  for (int wi = threadIdx.x; wi < CC * N; wi += NT) {
-    const int l = wi % CC, n = wi / CC;
-    s[n * LP + l] = base[(size_t)n * G::PITCH + l];
-  }
-  __syncthreads();
-  smem_fft<N, CC, NT, DIR>(s, tw);
-  for (int wi = threadIdx.x; wi < CC * N; wi += NT) {
-    const int l = wi % CC, n = wi / CC;
-    base[(size_t)n * G::PITCH + l] = s[n * LP + l];
-  }
-}
-
-// ---------------------------------------------------------------- z pass
-// Forward z FFT, psi = -psi/k2/(nx*ny*nz) with psi(0,0,0) = 0
-// (multi/main.f90:785-798), inverse z FFT, all in shared memory.
-// k2tab[m] holds kx(m)^2 (spectral) or (4/dx^2) sin^2(pi m/N) (FD-modified).
-template <int N, class T>
-__device__ __forceinline__ void zsolve_body(typename C2<T>::t* __restrict__ spec,
-                                            const typename C2<T>::t* __restrict__ tw,
-                                            const double* __restrict__ k2tab, const Ctrl* __restrict__ ctrl, int bx,
-                                            int by) {
-  typedef typename C2<T>::t C;
-  typedef PCfg<N, T> G;
-  constexpr int CC = G::CC, NT = G::NT;
-  if (ctrl && ctrl->status) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* s = reinterpret_cast<C*>(smem_raw);
-  const int jy = by;
-  const int m0 = bx * CC;
-  C* base = spec + (size_t)jy * G::PITCH + m0;
-  const size_t zstride = (size_t)N * G::PITCH;
-  constexpr int LP = Pitch<CC>::value;
-  for (int wi = threadIdx.x; wi < CC * N; wi += NT) {
-    const int l = wi % CC, n = wi / CC;
-    s[n * LP + l] = base[(size_t)n * zstride + l];
-  }
-  __syncthreads();
-  smem_fft<N, CC, NT, -1>(s, tw);
-  const double nnn = (double)((long long)N * (long long)N * (long long)N);
-  const double k2y = k2tab[jy];
-  for (int wi = threadIdx.x; wi < CC * N; wi += NT) {
-    const int l = wi % CC, n = wi / CC;
-    const int m = m0 + l;
-    C v = s[n * LP + l];
-    if (m > N / 2 || (m == 0 && jy == 0 && n == 0)) {
-      v.x = 0;
-      v.y = 0;
-    } else {
-      const double k2 = (k2tab[m] + k2y) + k2tab[n];
-      const double f = -1.0 / (k2 * nnn);
-      v.x = (T)((double)v.x * f);
-      v.y = (T)((double)v.y * f);
-    }
-    s[n * LP + l] = v;
-  }
-  __syncthreads();
-  smem_fft<N, CC, NT, +1>(s, tw);
-  for (int wi = threadIdx.x; wi < CC * N; wi += NT) {
-    const int l = wi % CC, n = wi / CC;
-    base[(size_t)n * zstride + l] = s[n * LP + l];
-  }
-}
-
 // ---------------------------------------------------------------- persistent column passes
 // The y passes and the z solve as persistent kernels: each CTA walks a
 // strided list of (column chunk, line) slabs.  The slab after the current one
@@ -403,18 +327,6 @@ __global__ void __launch_bounds__(256, 3) xfwd_kernel(const T* __restrict__ us, 
                                                   const Ctrl* __restrict__ ctrl, double cdiv, double ddxi) {
   xfwd_body<N, MODE, T>(us, vs, ws, rhs, p0, spec, tw, ctrl, cdiv, ddxi, blockIdx.x, blockIdx.y);
 }
-template <int N, int DIR, class T>
-__global__ void __launch_bounds__(256, 3) ypass_kernel(typename C2<T>::t* __restrict__ spec,
-                                                   const typename C2<T>::t* __restrict__ tw,
-                                                   const Ctrl* __restrict__ ctrl) {
-  ypass_body<N, DIR, T>(spec, tw, ctrl, blockIdx.x, blockIdx.y);
-}
-template <int N, class T>
-__global__ void __launch_bounds__(256, 3) zsolve_kernel(typename C2<T>::t* __restrict__ spec,
-                                                    const typename C2<T>::t* __restrict__ tw,
-                                                    const double* __restrict__ k2tab, const Ctrl* __restrict__ ctrl) {
-  zsolve_body<N, T>(spec, tw, k2tab, ctrl, blockIdx.x, blockIdx.y);
-}
 template <int N, class T>
 __global__ void __launch_bounds__(256, 3) xinv_kernel(const typename C2<T>::t* __restrict__ spec, T* __restrict__ p,
                                                   const typename C2<T>::t* __restrict__ tw,
@@ -432,20 +344,6 @@ __global__ void __launch_bounds__(256, 3) xfwd_kernel_b(const SlotArgs<T>* __res
   xfwd_body<N, MODE, T>(a.us, a.vs, a.ws, a.rhs, a.pres, a.spec, a.tw, a.ctrl, a.cdiv, a.ddxi, blockIdx.x,
                         blockIdx.y - sl * N);
 }
-template <int N, int DIR, class T>
-__global__ void __launch_bounds__(256, 3) ypass_kernel_b(const SlotArgs<T>* __restrict__ slots, int which) {
-  const int sl = blockIdx.y / N;
-  if (!slots[sl].active) return;
-  const PoissonArgs<T>& a = which ? slots[sl].pr : slots[sl].po;
-  ypass_body<N, DIR, T>(a.spec, a.tw, a.ctrl, blockIdx.x, blockIdx.y - sl * N);
-}
-template <int N, class T>
-__global__ void __launch_bounds__(256, 3) zsolve_kernel_b(const SlotArgs<T>* __restrict__ slots, int which) {
-  const int sl = blockIdx.y / N;
-  if (!slots[sl].active) return;
-  const PoissonArgs<T>& a = which ? slots[sl].pr : slots[sl].po;
-  zsolve_body<N, T>(a.spec, a.tw, a.k2tab, a.ctrl, blockIdx.x, blockIdx.y - sl * N);
-}
 template <int N, class T>
 __global__ void __launch_bounds__(256, 3) xinv_kernel_b(const SlotArgs<T>* __restrict__ slots, int which) {
   const int sl = blockIdx.y / N;
@@ -457,9 +355,6 @@ __global__ void __launch_bounds__(256, 3) xinv_kernel_b(const SlotArgs<T>* __res
 // ---------------------------------------------------------------- launchers
 template <int N, class T> static size_t xsmem() {
   return (size_t)N * Pitch<PCfg<N, T>::P>::value * sizeof(typename C2<T>::t);
-}
-template <int N, class T> static size_t csmem() {
-  return (size_t)N * Pitch<PCfg<N, T>::CC>::value * sizeof(typename C2<T>::t);
 }
 
 template <int N, class T> static size_t colsmem() {  // two slab buffers + the twiddle table
@@ -484,20 +379,14 @@ template <int N, int KIND, class T, bool BATCHED> static int colgrid() {
 
 template <int N, class T> static cudaError_t set_attrs() {
   cudaError_t e;
-  const int xs = (int)xsmem<N, T>(), cs = (int)csmem<N, T>();
+  const int xs = (int)xsmem<N, T>();
   if ((e = cudaFuncSetAttribute(xfwd_kernel<N, 0, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, xs))) return e;
   if ((e = cudaFuncSetAttribute(xfwd_kernel<N, 1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, xs))) return e;
   if ((e = cudaFuncSetAttribute(xfwd_kernel<N, 2, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, xs))) return e;
   if ((e = cudaFuncSetAttribute(xinv_kernel<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, xs))) return e;
-  if ((e = cudaFuncSetAttribute(ypass_kernel<N, -1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, cs))) return e;
-  if ((e = cudaFuncSetAttribute(ypass_kernel<N, 1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, cs))) return e;
-  if ((e = cudaFuncSetAttribute(zsolve_kernel<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, cs))) return e;
   if ((e = cudaFuncSetAttribute(xfwd_kernel_b<N, 0, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, xs))) return e;
   if ((e = cudaFuncSetAttribute(xfwd_kernel_b<N, 2, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, xs))) return e;
   if ((e = cudaFuncSetAttribute(xinv_kernel_b<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, xs))) return e;
-  if ((e = cudaFuncSetAttribute(ypass_kernel_b<N, -1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, cs))) return e;
-  if ((e = cudaFuncSetAttribute(ypass_kernel_b<N, 1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, cs))) return e;
-  if ((e = cudaFuncSetAttribute(zsolve_kernel_b<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, cs))) return e;
   const int ps = (int)colsmem<N, T>();
   if ((e = cudaFuncSetAttribute(colpass_kernel<N, 0, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps))) return e;
   if ((e = cudaFuncSetAttribute(colpass_kernel<N, 1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps))) return e;
@@ -527,10 +416,8 @@ static void launch_xfwd(const PoissonArgs<T>& a, cudaStream_t st) {
 template <int N, class T>
 static cudaError_t poisson_run(const PoissonArgs<T>& a, cudaStream_t st) {
   typedef PCfg<N, T> G;
-  const dim3 gx(N / (2 * G::P), N), gc(G::NCHUNK, N);
-  const size_t xs = xsmem<N, T>(), cs = csmem<N, T>();
-  (void)gc;
-  (void)cs;
+  const dim3 gx(N / (2 * G::P), N);
+  const size_t xs = xsmem<N, T>();
   const size_t ps = colsmem<N, T>();
   launch_xfwd<N, T>(a, st);
   colpass_kernel<N, 0, T><<<colgrid<N, 0, T, false>(), G::NT, ps, st>>>(a.spec, a.tw, a.k2tab, a.ctrl);
@@ -543,8 +430,8 @@ static cudaError_t poisson_run(const PoissonArgs<T>& a, cudaStream_t st) {
 template <int N, class T>
 static cudaError_t poisson_stage(const PoissonArgs<T>& a, int stage, cudaStream_t st) {
   typedef PCfg<N, T> G;
-  const dim3 gx(N / (2 * G::P), N), gc(G::NCHUNK, N);
-  const size_t xs = xsmem<N, T>(), cs = csmem<N, T>();
+  const dim3 gx(N / (2 * G::P), N);
+  const size_t xs = xsmem<N, T>();
   switch (stage) {
     case 0: launch_xfwd<N, T>(a, st); break;
     case 1:
@@ -583,8 +470,8 @@ template cudaError_t launch_poisson_stage<float>(int, const PoissonArgs<float>&,
 template <int N, class T>
 static cudaError_t poisson_stage_b(const SlotArgs<T>* slots, int nslots, int stage, int which, cudaStream_t st) {
   typedef PCfg<N, T> G;
-  const dim3 gx(N / (2 * G::P), N * nslots), gc(G::NCHUNK, N * nslots);
-  const size_t xs = xsmem<N, T>(), cs = csmem<N, T>();
+  const dim3 gx(N / (2 * G::P), N * nslots);
+  const size_t xs = xsmem<N, T>();
   switch (stage) {
     case 0:
       if (which)
