@@ -150,6 +150,7 @@ def main():
     t = time.perf_counter()
     build_inputs(reqs)
     gen_s = time.perf_counter() - t
+    step_s = {}  # plain FP64 device time per step of each (n, ACDI) class
     # warm the library: module loading of every kernel the stream uses is a
     # one-time process cost, not part of a request (tile autotuning is, and
     # the timed ensembles below start with fresh classes)
@@ -160,6 +161,9 @@ def main():
             with Solver(n, params(reqs[0], "fp64"), phase_field=pf) as s:
                 s.set_fields(*case, phi if pf else None)
                 s.step(2)
+                t = time.perf_counter()
+                s.step(20)  # returns after the device finished (diagnostics read back)
+                step_s[(n, pf)] = (time.perf_counter() - t) / 20
     with Ensemble(slots_per_class=a.slots) as ens:
         for n in sizes:
             case = [raw(x) for x in fields.random_velocity(n, 1)]
@@ -170,6 +174,9 @@ def main():
         ens.run()
     service = np.array(sequential(reqs))
     total_steps = sum(r["steps"] for r in reqs)
+    # what the stream costs the device alone, one request after another: the
+    # bound a server reaches by hiding all host work without batching gains
+    device_s = sum(r["steps"] * step_s[(r["n"], r["pf"])] for r in reqs)
     rate = a.load * len(reqs) / service.sum()  # requests per second offered
     arrivals = np.cumsum(gaps) / rate
     arrivals -= arrivals[0]
@@ -188,7 +195,8 @@ def main():
                 "bitwise_same_as_alone": (sum(same), len(same)) if same else None,
                 "ensemble": {"slots_per_class": a.slots, "classes": st["classes"], "rounds": st["rounds"],
                              "graph_launches": st["graph_launches"]},
-                "sizes": sizes, "input_generation_s": gen_s}
+                "sizes": sizes, "input_generation_s": gen_s,
+                "device_only_plain_steps_per_s": total_steps / device_s}
         print(json.dumps(line), flush=True)
 
 
