@@ -236,6 +236,24 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def max_over_ranks(x: float, world: int, device="cuda") -> float:
+    """The slowest rank's time: all-reduce MAX over the process group (every
+    rank takes part; world == 1 returns x)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replicas_rate(world: int, npts: int, steps: int, seconds: float) -> float:
+    """Whole-job Mpts*steps/s of `world` independent replicas, each doing
+    `steps` steps of `npts` points, timed by the slowest rank."""
+    return world * npts * steps / seconds / 1e6
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -281,11 +299,8 @@ def main():
     clk = clocks.stop()
     ms = e0.elapsed_time(e1)
     diag = s.diag()
-    if world > 1:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * n ** 3 * args.steps / (ms / 1e3) / 1e6
+    ms = max_over_ranks(ms, world)
+    value = replicas_rate(world, n ** 3, args.steps, ms / 1e3)
     launches = s.launches_per_step() * args.steps
 
     # per-kernel durations (individually launched, CUDA events on the stream)
@@ -326,12 +341,9 @@ def main():
         s.get_fields_ptr(*ptr)
         torch.cuda.synchronize()
         el = time.perf_counter() - t0
-        if world > 1:
-            t = torch.tensor([el], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            el = float(t.item())
+        el = max_over_ranks(el, world)
         nf = len(hb)
-        e2e = {"value": world * npts * args.steps / el / 1e6, "unit": UNIT,
+        e2e = {"value": replicas_rate(world, npts, args.steps, el), "unit": UNIT,
                "h2d_bytes_per_step": nf * npts * 8 / args.steps,
                "d2h_bytes_per_step": nf * npts * 8 / args.steps + 88,
                "ms_per_step": el / args.steps * 1e3}
