@@ -356,7 +356,9 @@ def main():
 
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "metric": METRIC if (args.precision == "fp64" and n == 512 and pf)
+            else f"Mpts*steps/s at {n}^3 NS{'+ACDI' if pf else ''} ({args.precision} form)",
+            "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32",
             "data": "synthetic (seeded random-phase velocity E(k)~k^4exp(-2(k/4)^2), seeded drops)",
