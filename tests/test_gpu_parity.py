@@ -126,7 +126,7 @@ def test_poisson_vs_oracle_random_rhs():
     from oracle import Oracle
     from mhit36_b200 import Solver
     rng = np.random.default_rng(7)
-    for n in (32, 64, 192):
+    for n in (32, 64, 96, 192, 384):
         rhs = rng.standard_normal((n, n, n))
         o = Oracle(n, phase_field=0)
         ref = o.poisson(rhs)
@@ -251,3 +251,26 @@ def test_poisson_manufactured_large(n):
         p = np.sin(x)[:, None, None] * np.cos(2 * x)[None, :, None] * np.sin(3 * x)[None, None, :]
         got = s.poisson(-14.0 * p)
     assert np.max(np.abs(got - p)) < 1e-12
+
+
+@pytest.mark.parametrize("n,pf,steps", [(96, True, 5), (192, False, 3)])
+def test_mixed_radix_sizes_vs_oracle(n, pf, steps):
+    """Sizes whose FFT plans use radix 3 (96 = 8*4*3, 192 = 8*8*3)."""
+    p = _params()
+    case = _case(n, True, ndrops=4, rmin=0.4, rmax=0.6) if pf else None
+    ref, got, _, _, _, _ = run_pair(n, steps, pf, p, case=case)
+    _check(ref, got, pf)
+
+
+@pytest.mark.parametrize("n", [32, 64, 96, 128, 192])
+def test_fp32_refinement_converges_at_every_size(n):
+    """max|div u| of the FP32 form's FP64 projection <= 1e-10 at each built size
+    up to 192^3 (each size has its own FFT chunking and x-pass configuration)."""
+    from mhit36_b200 import Solver, fields
+    p = _params(k2_mode=1)
+    u, v, w = fields.random_velocity(n, 11)
+    c, r = fields.place_drops(n, 12, 2, 0.4, 0.6)
+    with Solver(n, p, precision="fp32", phase_field=True) as s:
+        s.set_fields(u, v, w, fields.drop_field(n, c, r))
+        d = s.step(4)
+    assert d["max_div"] <= 1e-10, d["max_div"]
