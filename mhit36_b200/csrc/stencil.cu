@@ -82,8 +82,12 @@ __device__ __forceinline__ void phase_body(const StencilArgs<T>& a, int KZ, int 
   const int use_ident = a.c.tanh_identity;
   const T floor0 = a.c.phi_floor ? (T)0 : (T)-INFINITY;
   const T inv12e = (T)1 / ((T)1 + (T)2 * enumv);
-  // psi where min(phi,1) is exactly 0 (far field) or 1 (drop interiors): the
-  // same expression evaluated once, so skipping the log there changes nothing.
+  // psi where min(phi,1) is exactly 1 (drop interiors) or so small that both
+  // val + enum == enum and 1 - val + enum == 1 - 0 + enum in floating point
+  // (far field; the first implies the second, since it needs |val| below
+  // half an ulp of enum, far under 2^-54): there the reference's expression
+  // evaluates to psi1 / psi0 exactly, so those constants are computed once
+  // and the log is skipped -- bitwise the same values.
   const T psi0 = eps * log(((T)0 + enumv) / ((T)1 - (T)0 + enumv));
   const T psi1 = eps * log(((T)1 + enumv) / ((T)1 - (T)1 + enumv));
   const int x0 = bx * TX, y0 = by * TY, k0 = bz * KZ;
@@ -150,7 +154,8 @@ __device__ __forceinline__ void phase_body(const StencilArgs<T>& a, int KZ, int 
       const int e = tid + r * NT;
       if (r < NPE - 1 || e < PE) {
         const T val = fmax(fmin(Ph0[e], (T)1), floor0);
-        PsW[e] = (val == (T)0) ? psi0 : ((val == (T)1) ? psi1 : eps * log((val + enumv) / ((T)1 - val + enumv)));
+        PsW[e] = (val + enumv == enumv) ? psi0
+                 : ((val == (T)1) ? psi1 : eps * log((val + enumv) / ((T)1 - val + enumv)));
       }
     }
     __syncthreads();
