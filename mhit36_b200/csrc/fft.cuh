@@ -158,6 +158,71 @@ template <int N, int NS, int L, int NT, int DIR, class C> struct FFTRun {
   }
 };
 
+// ---------------------------------------------------------------- register-resident lines
+// Power-of-two N: a line is spread over TPC = N/8 threads, each holding eight
+// of its elements in registers, v[m] = x[t + TPC*m] for thread t of the line.
+// Every stage's butterflies run on registers -- butterfly b of the thread is
+// j = t + TPC*b with inputs v[b + (8/R)*r], which are x[j + r*N/R], the
+// Stockham map of fft_stage -- and the data crosses shared memory only
+// between stages: a stage writes its outputs at their Stockham positions and
+// the next stage reads the canonical v[m] back.  The last stage's outputs are
+// the canonical positions themselves (NS*R = N makes them x[j + r*N/R]), so
+// they stay in registers.  Each element sees fft_stage's arithmetic in the
+// same order, so both transforms give the same bits.
+//
+// Exchange buffer: CC lines interleaved, element n of line c at
+// s[(n + n/8)*CC + c].  The pad row after every 8 rows keeps a stage's
+// stride-R writes free of bank conflicts when a row is narrower than 128
+// bytes (CC*sizeof(C) = 32 or 64 bytes).
+__host__ __device__ constexpr int reg_rows(int N) { return N + N / 8; }
+
+template <int N, int NS, int CC, int DIR, class C>
+__device__ __forceinline__ void reg_fft_stages(C (&v)[8], C* s, const C* __restrict__ tw, int c, int t) {
+  if constexpr (NS < N) {
+    constexpr int R = pick_radix(N / NS);
+    static_assert(8 % R == 0, "register-resident lines need a power-of-two length");
+    constexpr int B = 8 / R, TPC = N / 8, TSTRIDE = N / (NS * R);
+#pragma unroll
+    for (int b = 0; b < B; ++b) {
+      const int j = t + TPC * b;
+      const int jm = j % NS;
+      C u[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        C a = v[b + B * r];
+        if (NS > 1 && r > 0) {
+          const C w = tw[r * jm * TSTRIDE];
+          a = (DIR < 0) ? cmul(a, w) : cmulc(a, w);
+        }
+        u[r] = a;
+      }
+      DFT<R, DIR, C>::run(u);
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[b + B * r] = u[r];
+    }
+    if constexpr (NS * R < N) {
+#pragma unroll
+      for (int b = 0; b < B; ++b) {
+        const int j = t + TPC * b;
+        const int d0 = (j / NS) * NS * R + j % NS;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int d = d0 + r * NS;
+          s[(d + (d >> 3)) * CC + c] = v[b + B * r];
+        }
+      }
+      __syncthreads();
+#pragma unroll
+      for (int m = 0; m < 8; ++m) {
+        const int n = t + TPC * m;
+        v[m] = s[(n + (n >> 3)) * CC + c];
+      }
+      __syncthreads();
+      reg_fft_stages<N, NS * R, CC, DIR, C>(v, s, tw, c, t);
+    }
+  }
+}
+
 // In-place transform of L interleaved lines of length N held in s.
 // Must be called by all NT threads of the CTA; ends with a barrier.
 template <int N, int L, int NT, int DIR, class C>

@@ -276,6 +276,115 @@ __global__ void __launch_bounds__(256, 2) colpass_kernel_b(const SlotArgs<T>* __
   });
 }
 
+// ---------------------------------------------------------------- register column passes
+// Power-of-two N: the y passes and the z solve on register-resident lines
+// (reg_fft_stages).  A CTA of CC*N/8 threads holds a slab of CC kx columns;
+// thread (c, t) loads the eight elements t + (N/8)*m of column c straight
+// from HBM into registers and stores them back from registers, and in the z
+// solve the -1/(k^2 N^3) scaling and the first inverse stage run on the
+// registers the forward transform left.  Shared memory carries only the
+// exchanges between stages: 4 accesses per element for a y pass at 512^3
+// (10 through the staged transform) and 8 for the z solve (18).  Latency is
+// hidden by the eight independent loads per thread and by the other
+// resident CTAs; the CTAs are persistent so that the twiddle table is
+// copied to shared memory once per CTA.
+template <int N, class T> struct RCfg {
+  static constexpr int CC = PCfg<N, T>::CC;
+  static constexpr int NT = CC * (N / 8);
+#ifdef MHIT_STAGED_COLUMNS
+  static constexpr bool ON = false;
+#else
+  static constexpr bool ON = (N & (N - 1)) == 0;
+#endif
+};
+
+template <int N, class T> static size_t rcolsmem() {  // exchange buffer + the twiddle table
+  return ((size_t)reg_rows(N) * RCfg<N, T>::CC + N) * sizeof(typename C2<T>::t);
+}
+
+template <int N, int KIND, class T, class Getter>
+__device__ __forceinline__ void rcol_run(int total, const typename C2<T>::t* __restrict__ gtw, Getter get) {
+  typedef typename C2<T>::t C;
+  constexpr int CC = RCfg<N, T>::CC, TPC = N / 8;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* s = reinterpret_cast<C*>(smem_raw);
+  C* stw = s + reg_rows(N) * CC;
+  if ((int)blockIdx.x >= total) return;
+  for (int q = threadIdx.x; q < N; q += RCfg<N, T>::NT) stw[q] = gtw[q];
+  __syncthreads();
+  const int c = threadIdx.x % CC, t = threadIdx.x / CC;
+  for (int it = blockIdx.x; it < total; it += gridDim.x) {
+    const ColSlab sl = get(it);
+    if (!sl.live) continue;  // the same for every thread of the CTA
+    C* col = static_cast<C*>(sl.spec) + c;
+    C v[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) v[m] = col[(size_t)(t + TPC * m) * sl.stride];
+    if (KIND == 0) {
+      reg_fft_stages<N, 1, CC, -1>(v, s, stw, c, t);
+    } else if (KIND == 1) {
+      reg_fft_stages<N, 1, CC, +1>(v, s, stw, c, t);
+    } else {
+      // forward z FFT, then -psi/k2/(nx*ny*nz) per mode (multi/main.f90:792,
+      // one reciprocal per mode; mode (0,0,0) and the pitch padding beyond
+      // kx = N/2 set to 0), then the inverse z FFT
+      reg_fft_stages<N, 1, CC, -1>(v, s, stw, c, t);
+      const double nnn = (double)((long long)N * (long long)N * (long long)N);
+      const double* k2tab = sl.k2tab;
+      const int mx = sl.m0 + c, jy = sl.jy;
+      const double k2xy = k2tab[min(mx, N - 1)] + k2tab[jy];
+#pragma unroll
+      for (int m = 0; m < 8; ++m) {
+        const int n = t + TPC * m;
+        if (mx > N / 2 || (mx == 0 && jy == 0 && n == 0)) {
+          v[m].x = 0;
+          v[m].y = 0;
+        } else {
+          const double k2 = k2xy + k2tab[n];
+          const double f = -1.0 / (k2 * nnn);
+          v[m].x = (T)((double)v[m].x * f);
+          v[m].y = (T)((double)v[m].y * f);
+        }
+      }
+      reg_fft_stages<N, 1, CC, +1>(v, s, stw, c, t);
+    }
+#pragma unroll
+    for (int m = 0; m < 8; ++m) col[(size_t)(t + TPC * m) * sl.stride] = v[m];
+  }
+}
+
+template <int N, int KIND, class T>
+__global__ void __launch_bounds__(RCfg<N, T>::NT) rcol_kernel(typename C2<T>::t* __restrict__ spec,
+                                                              const typename C2<T>::t* __restrict__ tw,
+                                                              const double* __restrict__ k2tab,
+                                                              const Ctrl* __restrict__ ctrl) {
+  typedef PCfg<N, T> G;
+  rcol_run<N, KIND, T>(G::NCHUNK * N, tw,
+                       [&](int it) { return slab_single<N, KIND, T>(spec, tw, k2tab, ctrl, it); });
+}
+
+template <int N, int KIND, class T>
+__global__ void __launch_bounds__(RCfg<N, T>::NT) rcol_kernel_b(const SlotArgs<T>* __restrict__ slots, int nslots,
+                                                                int which) {
+  typedef PCfg<N, T> G;
+  const int per = G::NCHUNK * N;
+  const typename C2<T>::t* tw = nullptr;
+  for (int q = 0; q < nslots && !tw; ++q)
+    if (slots[q].active) tw = (which ? slots[q].pr : slots[q].po).tw;
+  if (!tw) return;
+  rcol_run<N, KIND, T>(per * nslots, tw, [&](int it) {
+    const int sl = it / per;
+    const PoissonArgs<T>& a = which ? slots[sl].pr : slots[sl].po;
+    ColSlab s;
+    if (!slots[sl].active) {
+      s.live = false;
+      return s;
+    }
+    s = slab_single<N, KIND, T>(a.spec, a.tw, a.k2tab, a.ctrl, it - sl * per);
+    return s;
+  });
+}
+
 // ---------------------------------------------------------------- x inverse
 // Complex-to-real x transform of two lines at once; writes p
 // (multi/main.f90:812, 842-850: p = real(psi)).
@@ -411,6 +520,43 @@ template <int N, int KIND, class T, bool BATCHED> static int colgrid() {
   return grid;
 }
 
+// The same for the register column passes.
+template <int N, int KIND, class T, bool BATCHED> static int rcolgrid() {
+  static int grid = 0;
+  if (!grid) {
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (BATCHED)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, rcol_kernel_b<N, KIND, T>, RCfg<N, T>::NT,
+                                                    rcolsmem<N, T>());
+    else
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, rcol_kernel<N, KIND, T>, RCfg<N, T>::NT, rcolsmem<N, T>());
+    grid = std::max(1, sms) * std::max(1, per);
+  }
+  return grid;
+}
+
+// Column pass KIND of one solve / of the slots of an ensemble class: the
+// register-resident transform for power-of-two N, the staged one otherwise.
+template <int N, int KIND, class T> static void launch_col(const PoissonArgs<T>& a, cudaStream_t st) {
+  if constexpr (RCfg<N, T>::ON)
+    rcol_kernel<N, KIND, T><<<rcolgrid<N, KIND, T, false>(), RCfg<N, T>::NT, rcolsmem<N, T>(), st>>>(
+        a.spec, a.tw, a.k2tab, a.ctrl);
+  else
+    colpass_kernel<N, KIND, T><<<colgrid<N, KIND, T, false>(), PCfg<N, T>::NT, colsmem<N, T>(), st>>>(
+        a.spec, a.tw, a.k2tab, a.ctrl);
+}
+template <int N, int KIND, class T>
+static void launch_col_b(const SlotArgs<T>* slots, int nslots, int which, cudaStream_t st) {
+  if constexpr (RCfg<N, T>::ON)
+    rcol_kernel_b<N, KIND, T><<<rcolgrid<N, KIND, T, true>(), RCfg<N, T>::NT, rcolsmem<N, T>(), st>>>(
+        slots, nslots, which);
+  else
+    colpass_kernel_b<N, KIND, T><<<colgrid<N, KIND, T, true>(), PCfg<N, T>::NT, colsmem<N, T>(), st>>>(
+        slots, nslots, which);
+}
+
 template <int N, class T> static cudaError_t set_attrs() {
   cudaError_t e;
   const int xs = (int)xsmem<N, T>();
@@ -428,6 +574,15 @@ template <int N, class T> static cudaError_t set_attrs() {
   if ((e = cudaFuncSetAttribute(colpass_kernel_b<N, 0, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps))) return e;
   if ((e = cudaFuncSetAttribute(colpass_kernel_b<N, 1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps))) return e;
   if ((e = cudaFuncSetAttribute(colpass_kernel_b<N, 2, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps))) return e;
+  if constexpr (RCfg<N, T>::ON) {
+    const int rs = (int)rcolsmem<N, T>();
+    if ((e = cudaFuncSetAttribute(rcol_kernel<N, 0, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, rs))) return e;
+    if ((e = cudaFuncSetAttribute(rcol_kernel<N, 1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, rs))) return e;
+    if ((e = cudaFuncSetAttribute(rcol_kernel<N, 2, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, rs))) return e;
+    if ((e = cudaFuncSetAttribute(rcol_kernel_b<N, 0, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, rs))) return e;
+    if ((e = cudaFuncSetAttribute(rcol_kernel_b<N, 1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, rs))) return e;
+    if ((e = cudaFuncSetAttribute(rcol_kernel_b<N, 2, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, rs))) return e;
+  }
   return cudaSuccess;
 }
 
@@ -452,11 +607,10 @@ static cudaError_t poisson_run(const PoissonArgs<T>& a, cudaStream_t st) {
   typedef PCfg<N, T> G;
   const dim3 gx(N / (2 * G::P), N);
   const size_t xs = xsmem<N, T>();
-  const size_t ps = colsmem<N, T>();
   launch_xfwd<N, T>(a, st);
-  colpass_kernel<N, 0, T><<<colgrid<N, 0, T, false>(), G::NT, ps, st>>>(a.spec, a.tw, a.k2tab, a.ctrl);
-  colpass_kernel<N, 2, T><<<colgrid<N, 2, T, false>(), G::NT, ps, st>>>(a.spec, a.tw, a.k2tab, a.ctrl);
-  colpass_kernel<N, 1, T><<<colgrid<N, 1, T, false>(), G::NT, ps, st>>>(a.spec, a.tw, a.k2tab, a.ctrl);
+  launch_col<N, 0, T>(a, st);
+  launch_col<N, 2, T>(a, st);
+  launch_col<N, 1, T>(a, st);
   xinv_kernel<N, T><<<gx, G::NT, xs, st>>>(a.spec, a.p, a.tw, a.ctrl);
   return cudaGetLastError();
 }
@@ -468,18 +622,9 @@ static cudaError_t poisson_stage(const PoissonArgs<T>& a, int stage, cudaStream_
   const size_t xs = xsmem<N, T>();
   switch (stage) {
     case 0: launch_xfwd<N, T>(a, st); break;
-    case 1:
-      colpass_kernel<N, 0, T><<<colgrid<N, 0, T, false>(), G::NT, colsmem<N, T>(), st>>>(a.spec, a.tw, a.k2tab,
-                                                                                       a.ctrl);
-      break;
-    case 2:
-      colpass_kernel<N, 2, T><<<colgrid<N, 2, T, false>(), G::NT, colsmem<N, T>(), st>>>(a.spec, a.tw, a.k2tab,
-                                                                                       a.ctrl);
-      break;
-    case 3:
-      colpass_kernel<N, 1, T><<<colgrid<N, 1, T, false>(), G::NT, colsmem<N, T>(), st>>>(a.spec, a.tw, a.k2tab,
-                                                                                       a.ctrl);
-      break;
+    case 1: launch_col<N, 0, T>(a, st); break;
+    case 2: launch_col<N, 2, T>(a, st); break;
+    case 3: launch_col<N, 1, T>(a, st); break;
     case 4: xinv_kernel<N, T><<<gx, G::NT, xs, st>>>(a.spec, a.p, a.tw, a.ctrl); break;
     default: return cudaErrorInvalidValue;
   }
@@ -513,9 +658,9 @@ static cudaError_t poisson_stage_b(const SlotArgs<T>* slots, int nslots, int sta
       else
         xfwd_kernel_b<N, 0, T><<<gx, G::NT, xs, st>>>(slots, 0);
       break;
-    case 1: colpass_kernel_b<N, 0, T><<<colgrid<N, 0, T, true>(), G::NT, colsmem<N, T>(), st>>>(slots, nslots, which); break;
-    case 2: colpass_kernel_b<N, 2, T><<<colgrid<N, 2, T, true>(), G::NT, colsmem<N, T>(), st>>>(slots, nslots, which); break;
-    case 3: colpass_kernel_b<N, 1, T><<<colgrid<N, 1, T, true>(), G::NT, colsmem<N, T>(), st>>>(slots, nslots, which); break;
+    case 1: launch_col_b<N, 0, T>(slots, nslots, which, st); break;
+    case 2: launch_col_b<N, 2, T>(slots, nslots, which, st); break;
+    case 3: launch_col_b<N, 1, T>(slots, nslots, which, st); break;
     case 4: xinv_kernel_b<N, T><<<gx, G::NT, xs, st>>>(slots, which); break;
     default: return cudaErrorInvalidValue;
   }
