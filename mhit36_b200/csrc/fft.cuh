@@ -170,14 +170,16 @@ template <int N, int NS, int L, int NT, int DIR, class C> struct FFTRun {
 // they stay in registers.  Each element sees fft_stage's arithmetic in the
 // same order, so both transforms give the same bits.
 //
-// Exchange buffer: CC lines interleaved, element n of line c at
-// s[(n + n/8)*CC + c].  The pad row after every 8 rows keeps a stage's
-// stride-R writes free of bank conflicts when a row is narrower than 128
-// bytes (CC*sizeof(C) = 32 or 64 bytes).
+// Exchange buffer: `at(n)` is the shared-memory slot of element n of the
+// thread's line.  Both layouts in use pad one element after every 8
+// (n + n/8), which keeps a stage's stride-R writes free of bank conflicts:
+// lines interleaved (element n of line c at (n + n/8)*CC + c, for column
+// slabs whose rows are narrower than 128 bytes) or one line after another
+// (line c at c*reg_rows(N) + n + n/8, for x lines).
 __host__ __device__ constexpr int reg_rows(int N) { return N + N / 8; }
 
-template <int N, int NS, int CC, int DIR, class C>
-__device__ __forceinline__ void reg_fft_stages(C (&v)[8], C* s, const C* __restrict__ tw, int c, int t) {
+template <int N, int NS, int DIR, class C, class At>
+__device__ __forceinline__ void reg_fft_stages(C (&v)[8], C* s, const C* __restrict__ tw, int t, const At& at) {
   if constexpr (NS < N) {
     constexpr int R = pick_radix(N / NS);
     static_assert(8 % R == 0, "register-resident lines need a power-of-two length");
@@ -207,18 +209,14 @@ __device__ __forceinline__ void reg_fft_stages(C (&v)[8], C* s, const C* __restr
         const int d0 = (j / NS) * NS * R + j % NS;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-          const int d = d0 + r * NS;
-          s[(d + (d >> 3)) * CC + c] = v[b + B * r];
+          s[at(d0 + r * NS)] = v[b + B * r];
         }
       }
       __syncthreads();
 #pragma unroll
-      for (int m = 0; m < 8; ++m) {
-        const int n = t + TPC * m;
-        v[m] = s[(n + (n >> 3)) * CC + c];
-      }
+      for (int m = 0; m < 8; ++m) v[m] = s[at(t + TPC * m)];
       __syncthreads();
-      reg_fft_stages<N, NS * R, CC, DIR, C>(v, s, tw, c, t);
+      reg_fft_stages<N, NS * R, DIR, C>(v, s, tw, t, at);
     }
   }
 }

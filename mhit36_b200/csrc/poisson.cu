@@ -284,10 +284,9 @@ __global__ void __launch_bounds__(256, 2) colpass_kernel_b(const SlotArgs<T>* __
 // solve the -1/(k^2 N^3) scaling and the first inverse stage run on the
 // registers the forward transform left.  Shared memory carries only the
 // exchanges between stages: 4 accesses per element for a y pass at 512^3
-// (10 through the staged transform) and 8 for the z solve (18).  Latency is
-// hidden by the eight independent loads per thread and by the other
-// resident CTAs; the CTAs are persistent so that the twiddle table is
-// copied to shared memory once per CTA.
+// (10 through the staged transform) and 8 for the z solve (18).  The CTAs
+// are persistent, so that the twiddle table is copied to shared memory once
+// per CTA.
 template <int N, class T> struct RCfg {
   static constexpr int CC = PCfg<N, T>::CC;
   static constexpr int NT = CC * (N / 8);
@@ -296,10 +295,26 @@ template <int N, class T> struct RCfg {
 #else
   static constexpr bool ON = (N & (N - 1)) == 0;
 #endif
+  // Resident CTAs per SM the kernels are built for: registers capped at 80
+  // per thread in FP64 (3 CTAs of 256 threads), 64 in the FP32 y passes and
+  // 40 in the FP32 z solve (measured on B200 at 512^3: the FP32 z solve
+  // 0.68 -> 0.57 ms at 40; uncapped or lower caps were slower elsewhere).
+  // FP64: the next slab is prefetched into shared memory with cp.async while
+  // the current one is transformed (512^3: y passes 0.48 -> 0.41 ms, z solve
+  // 0.94 -> 0.88 ms); the FP32 passes are faster without (0.24 vs 0.25 and
+  // 0.56 vs 0.66 ms), their extra buffer costing resident CTAs.  The twiddle
+  // table sits in shared memory (reading it through L1 measured slower).
+  static constexpr bool PF = sizeof(T) == 8;
+  static constexpr bool STW = true;
+  static constexpr int minb(int kind) {
+    const int r = sizeof(T) == 8 ? (kind == 2 ? 128 : 80) : (kind == 2 ? 40 : 64);
+    return 65536 / (NT * r) > 1 ? 65536 / (NT * r) : 1;
+  }
 };
 
-template <int N, class T> static size_t rcolsmem() {  // exchange buffer + the twiddle table
-  return ((size_t)reg_rows(N) * RCfg<N, T>::CC + N) * sizeof(typename C2<T>::t);
+template <int N, class T> static size_t rcolsmem() {  // exchange buffer, twiddle table, prefetch buffer
+  typedef RCfg<N, T> R;
+  return ((size_t)reg_rows(N) * R::CC + (R::STW ? N : 0) + (R::PF ? 8 * R::NT : 0)) * sizeof(typename C2<T>::t);
 }
 
 template <int N, int KIND, class T, class Getter>
@@ -307,28 +322,65 @@ __device__ __forceinline__ void rcol_run(int total, const typename C2<T>::t* __r
   typedef typename C2<T>::t C;
   constexpr int CC = RCfg<N, T>::CC, TPC = N / 8;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int NT = RCfg<N, T>::NT;
   C* s = reinterpret_cast<C*>(smem_raw);
   C* stw = s + reg_rows(N) * CC;
+  C* pbuf = stw + (RCfg<N, T>::STW ? N : 0);
   if ((int)blockIdx.x >= total) return;
-  for (int q = threadIdx.x; q < N; q += RCfg<N, T>::NT) stw[q] = gtw[q];
-  __syncthreads();
+  const C* tw = gtw;
+  if constexpr (RCfg<N, T>::STW) {
+    for (int q = threadIdx.x; q < N; q += NT) stw[q] = gtw[q];
+    __syncthreads();
+    tw = stw;
+  }
   const int c = threadIdx.x % CC, t = threadIdx.x / CC;
-  for (int it = blockIdx.x; it < total; it += gridDim.x) {
-    const ColSlab sl = get(it);
-    if (!sl.live) continue;  // the same for every thread of the CTA
-    C* col = static_cast<C*>(sl.spec) + c;
-    C v[8];
+  const auto at = [c](int n) { return (n + (n >> 3)) * CC + c; };
+  // prefetch: each thread copies its own eight elements of the next slab into
+  // its own slots (m*NT + tid), so only its own cp.async wait orders them
+  auto prefetch = [&](const ColSlab& ps) {
+    if (ps.live) {
+      const C* pc = static_cast<const C*>(ps.spec) + c;
 #pragma unroll
-    for (int m = 0; m < 8; ++m) v[m] = col[(size_t)(t + TPC * m) * sl.stride];
+      for (int m = 0; m < 8; ++m) cp_async_elem(pbuf + m * NT + threadIdx.x, pc + (size_t)(t + TPC * m) * ps.stride);
+    }
+    cp_async_commit();
+  };
+  ColSlab nx;
+  if constexpr (RCfg<N, T>::PF) {
+    nx = get(blockIdx.x);
+    prefetch(nx);
+  }
+  for (int it = blockIdx.x; it < total; it += gridDim.x) {
+    C v[8];
+    ColSlab sl;
+    if constexpr (RCfg<N, T>::PF) {
+      sl = nx;
+      cp_async_wait<0>();
+      if (sl.live) {
+#pragma unroll
+        for (int m = 0; m < 8; ++m) v[m] = pbuf[m * NT + threadIdx.x];
+      }
+      nx.live = false;
+      if (it + (int)gridDim.x < total) nx = get(it + gridDim.x);
+      prefetch(nx);
+      if (!sl.live) continue;
+    } else {
+      sl = get(it);
+      if (!sl.live) continue;  // the same for every thread of the CTA
+      const C* lc = static_cast<const C*>(sl.spec) + c;
+#pragma unroll
+      for (int m = 0; m < 8; ++m) v[m] = lc[(size_t)(t + TPC * m) * sl.stride];
+    }
+    C* col = static_cast<C*>(sl.spec) + c;
     if (KIND == 0) {
-      reg_fft_stages<N, 1, CC, -1>(v, s, stw, c, t);
+      reg_fft_stages<N, 1, -1>(v, s, tw, t, at);
     } else if (KIND == 1) {
-      reg_fft_stages<N, 1, CC, +1>(v, s, stw, c, t);
+      reg_fft_stages<N, 1, +1>(v, s, tw, t, at);
     } else {
       // forward z FFT, then -psi/k2/(nx*ny*nz) per mode (multi/main.f90:792,
       // one reciprocal per mode; mode (0,0,0) and the pitch padding beyond
       // kx = N/2 set to 0), then the inverse z FFT
-      reg_fft_stages<N, 1, CC, -1>(v, s, stw, c, t);
+      reg_fft_stages<N, 1, -1>(v, s, tw, t, at);
       const double nnn = (double)((long long)N * (long long)N * (long long)N);
       const double* k2tab = sl.k2tab;
       const int mx = sl.m0 + c, jy = sl.jy;
@@ -346,7 +398,7 @@ __device__ __forceinline__ void rcol_run(int total, const typename C2<T>::t* __r
           v[m].y = (T)((double)v[m].y * f);
         }
       }
-      reg_fft_stages<N, 1, CC, +1>(v, s, stw, c, t);
+      reg_fft_stages<N, 1, +1>(v, s, tw, t, at);
     }
 #pragma unroll
     for (int m = 0; m < 8; ++m) col[(size_t)(t + TPC * m) * sl.stride] = v[m];
@@ -354,7 +406,7 @@ __device__ __forceinline__ void rcol_run(int total, const typename C2<T>::t* __r
 }
 
 template <int N, int KIND, class T>
-__global__ void __launch_bounds__(RCfg<N, T>::NT) rcol_kernel(typename C2<T>::t* __restrict__ spec,
+__global__ void __launch_bounds__(RCfg<N, T>::NT, RCfg<N, T>::minb(KIND)) rcol_kernel(typename C2<T>::t* __restrict__ spec,
                                                               const typename C2<T>::t* __restrict__ tw,
                                                               const double* __restrict__ k2tab,
                                                               const Ctrl* __restrict__ ctrl) {
@@ -364,7 +416,7 @@ __global__ void __launch_bounds__(RCfg<N, T>::NT) rcol_kernel(typename C2<T>::t*
 }
 
 template <int N, int KIND, class T>
-__global__ void __launch_bounds__(RCfg<N, T>::NT) rcol_kernel_b(const SlotArgs<T>* __restrict__ slots, int nslots,
+__global__ void __launch_bounds__(RCfg<N, T>::NT, RCfg<N, T>::minb(KIND)) rcol_kernel_b(const SlotArgs<T>* __restrict__ slots, int nslots,
                                                                 int which) {
   typedef PCfg<N, T> G;
   const int per = G::NCHUNK * N;
@@ -460,6 +512,119 @@ __device__ __forceinline__ void xinv_body(const typename C2<T>::t* __restrict__ 
   }
 }
 
+// ---------------------------------------------------------------- register x passes
+// Power-of-two N: the x passes on register-resident lines (reg_fft_stages),
+// P*N/8 threads per CTA, thread (q, t) holding elements t + (N/8)*m of line
+// pair q.  x inverse: each thread reads the two half spectra at
+// min(n, N - n) for its own elements n straight into registers, so the
+// unpacking takes no shared-memory pass (the mirrored half reads a row
+// segment another warp reads too, an L1/L2 hit); the transformed line goes
+// from registers to p.  x forward: the divergence of each thread's
+// elements is computed straight into registers; the transformed line is
+// written once to shared memory for the Hermitian split, which needs modes
+// m and N - m together.
+template <int N, class T> struct XCfg {
+  static constexpr bool ON = RCfg<N, T>::ON;
+  static constexpr int NT = ON ? PCfg<N, T>::P * (N / 8) : PCfg<N, T>::NT;
+};
+
+template <int N, class T>
+__device__ __forceinline__ void xinv_reg_body(const typename C2<T>::t* __restrict__ spec, T* __restrict__ p,
+                                              const typename C2<T>::t* __restrict__ tw,
+                                              const Ctrl* __restrict__ ctrl, int bx, int by) {
+  typedef typename C2<T>::t C;
+  typedef PCfg<N, T> G;
+  constexpr int TPC = N / 8, RS = reg_rows(N);
+  if (ctrl && ctrl->status) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* s = reinterpret_cast<C*>(smem_raw);
+  const int t = threadIdx.x % TPC, q = threadIdx.x / TPC;
+  const int k = by, ja = bx * (2 * G::P) + 2 * q;
+  const C* row = spec + ((size_t)k * N + ja) * G::PITCH;
+  C A[8], B[8];
+#pragma unroll
+  for (int m = 0; m < 8; ++m) {
+    const int n = t + TPC * m;
+    const int h = (n <= N / 2) ? n : N - n;
+    A[m] = row[h];
+    B[m] = row[G::PITCH + h];
+  }
+  // z = A + iB on modes 0..N/2 and its Hermitian mirror above (the imaginary
+  // parts of modes 0 and N/2 dropped)
+  C v[8];
+#pragma unroll
+  for (int m = 0; m < 8; ++m) {
+    const int n = t + TPC * m;
+    C a = A[m], b = B[m];
+    if (n == 0 || n == N / 2) {
+      a.y = 0;
+      b.y = 0;
+    }
+    if (n <= N / 2) {
+      v[m].x = a.x - b.y;
+      v[m].y = a.y + b.x;
+    } else {
+      v[m].x = a.x + b.y;
+      v[m].y = b.x - a.y;
+    }
+  }
+  const int base = q * RS;
+  reg_fft_stages<N, 1, +1>(v, s, tw, t, [base](int n) { return base + n + (n >> 3); });
+#pragma unroll
+  for (int m = 0; m < 8; ++m) {
+    const int n = t + TPC * m;
+    p[gidx(n, ja, k, N)] = v[m].x;
+    p[gidx(n, ja + 1, k, N)] = v[m].y;
+  }
+}
+
+template <int N, int MODE, class T>
+__device__ __forceinline__ void xfwd_reg_body(const T* __restrict__ us, const T* __restrict__ vs,
+                                              const T* __restrict__ ws, const T* __restrict__ rhs,
+                                              const T* __restrict__ p0, typename C2<T>::t* __restrict__ spec,
+                                              const typename C2<T>::t* __restrict__ tw,
+                                              const Ctrl* __restrict__ ctrl, double cdiv, double ddxi, int bx,
+                                              int by) {
+  typedef typename C2<T>::t C;
+  typedef PCfg<N, T> G;
+  constexpr int TPC = N / 8, RS = reg_rows(N), M = N / 2 + 1;
+  if (ctrl && ctrl->status) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* s = reinterpret_cast<C*>(smem_raw);
+  const int t = threadIdx.x % TPC, q = threadIdx.x / TPC;
+  const int k = by, j0 = bx * (2 * G::P);
+  const int ja = j0 + 2 * q;
+  C v[8];
+#pragma unroll
+  for (int m = 0; m < 8; ++m) {
+    const int n = t + TPC * m;
+    v[m].x = (T)xfwd_rhs<N, MODE, T>(us, vs, ws, rhs, p0, cdiv, ddxi, n, ja, k);
+    v[m].y = (T)xfwd_rhs<N, MODE, T>(us, vs, ws, rhs, p0, cdiv, ddxi, n, ja + 1, k);
+  }
+  const int base = q * RS;
+  const auto at = [base](int n) { return base + n + (n >> 3); };
+  reg_fft_stages<N, 1, -1>(v, s, tw, t, at);
+#pragma unroll
+  for (int m = 0; m < 8; ++m) s[at(t + TPC * m)] = v[m];
+  __syncthreads();
+  const T half = (T)0.5;
+  for (int wi = threadIdx.x; wi < G::P * M; wi += XCfg<N, T>::NT) {
+    const int m = wi % M, pq = wi / M;
+    const int jb = j0 + 2 * pq;
+    const C zm = s[pq * RS + m + (m >> 3)];
+    const int mr = (m == 0) ? 0 : (N - m);
+    const C zr = s[pq * RS + mr + (mr >> 3)];
+    C Am, Bm;
+    Am.x = half * (zm.x + zr.x);
+    Am.y = half * (zm.y - zr.y);
+    Bm.x = half * (zm.y + zr.y);
+    Bm.y = -half * (zm.x - zr.x);
+    C* orow = spec + ((size_t)k * N + jb) * G::PITCH;
+    orow[m] = Am;
+    orow[G::PITCH + m] = Bm;
+  }
+}
+
 // ---------------------------------------------------------------- entry points
 // Single solve: block coordinates are the grid's.
 template <int N, int MODE, class T>
@@ -468,13 +633,19 @@ __global__ void __launch_bounds__(256, 3) xfwd_kernel(const T* __restrict__ us, 
                                                   const T* __restrict__ p0, typename C2<T>::t* __restrict__ spec,
                                                   const typename C2<T>::t* __restrict__ tw,
                                                   const Ctrl* __restrict__ ctrl, double cdiv, double ddxi) {
-  xfwd_body<N, MODE, T>(us, vs, ws, rhs, p0, spec, tw, ctrl, cdiv, ddxi, blockIdx.x, blockIdx.y);
+  if constexpr (XCfg<N, T>::ON)
+    xfwd_reg_body<N, MODE, T>(us, vs, ws, rhs, p0, spec, tw, ctrl, cdiv, ddxi, blockIdx.x, blockIdx.y);
+  else
+    xfwd_body<N, MODE, T>(us, vs, ws, rhs, p0, spec, tw, ctrl, cdiv, ddxi, blockIdx.x, blockIdx.y);
 }
 template <int N, class T>
 __global__ void __launch_bounds__(256, 3) xinv_kernel(const typename C2<T>::t* __restrict__ spec, T* __restrict__ p,
                                                   const typename C2<T>::t* __restrict__ tw,
                                                   const Ctrl* __restrict__ ctrl) {
-  xinv_body<N, T>(spec, p, tw, ctrl, blockIdx.x, blockIdx.y);
+  if constexpr (XCfg<N, T>::ON)
+    xinv_reg_body<N, T>(spec, p, tw, ctrl, blockIdx.x, blockIdx.y);
+  else
+    xinv_body<N, T>(spec, p, tw, ctrl, blockIdx.x, blockIdx.y);
 }
 
 // Batched over the slots of a served ensemble: grid y = slot * N + plane.
@@ -484,19 +655,27 @@ __global__ void __launch_bounds__(256, 3) xfwd_kernel_b(const SlotArgs<T>* __res
   const int sl = blockIdx.y / N;
   if (!slots[sl].active) return;
   const PoissonArgs<T>& a = which ? slots[sl].pr : slots[sl].po;
-  xfwd_body<N, MODE, T>(a.us, a.vs, a.ws, a.rhs, a.pres, a.spec, a.tw, a.ctrl, a.cdiv, a.ddxi, blockIdx.x,
-                        blockIdx.y - sl * N);
+  if constexpr (XCfg<N, T>::ON)
+    xfwd_reg_body<N, MODE, T>(a.us, a.vs, a.ws, a.rhs, a.pres, a.spec, a.tw, a.ctrl, a.cdiv, a.ddxi, blockIdx.x,
+                              blockIdx.y - sl * N);
+  else
+    xfwd_body<N, MODE, T>(a.us, a.vs, a.ws, a.rhs, a.pres, a.spec, a.tw, a.ctrl, a.cdiv, a.ddxi, blockIdx.x,
+                          blockIdx.y - sl * N);
 }
 template <int N, class T>
 __global__ void __launch_bounds__(256, 3) xinv_kernel_b(const SlotArgs<T>* __restrict__ slots, int which) {
   const int sl = blockIdx.y / N;
   if (!slots[sl].active) return;
   const PoissonArgs<T>& a = which ? slots[sl].pr : slots[sl].po;
-  xinv_body<N, T>(a.spec, a.p, a.tw, a.ctrl, blockIdx.x, blockIdx.y - sl * N);
+  if constexpr (XCfg<N, T>::ON)
+    xinv_reg_body<N, T>(a.spec, a.p, a.tw, a.ctrl, blockIdx.x, blockIdx.y - sl * N);
+  else
+    xinv_body<N, T>(a.spec, a.p, a.tw, a.ctrl, blockIdx.x, blockIdx.y - sl * N);
 }
 
 // ---------------------------------------------------------------- launchers
 template <int N, class T> static size_t xsmem() {
+  if constexpr (XCfg<N, T>::ON) return (size_t)PCfg<N, T>::P * reg_rows(N) * sizeof(typename C2<T>::t);
   return (size_t)N * Pitch<PCfg<N, T>::P>::value * sizeof(typename C2<T>::t);
 }
 
@@ -567,14 +746,15 @@ template <int N, class T> static cudaError_t set_attrs() {
   if ((e = cudaFuncSetAttribute(xfwd_kernel_b<N, 0, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, xs))) return e;
   if ((e = cudaFuncSetAttribute(xfwd_kernel_b<N, 2, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, xs))) return e;
   if ((e = cudaFuncSetAttribute(xinv_kernel_b<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, xs))) return e;
-  const int ps = (int)colsmem<N, T>();
-  if ((e = cudaFuncSetAttribute(colpass_kernel<N, 0, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps))) return e;
-  if ((e = cudaFuncSetAttribute(colpass_kernel<N, 1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps))) return e;
-  if ((e = cudaFuncSetAttribute(colpass_kernel<N, 2, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps))) return e;
-  if ((e = cudaFuncSetAttribute(colpass_kernel_b<N, 0, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps))) return e;
-  if ((e = cudaFuncSetAttribute(colpass_kernel_b<N, 1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps))) return e;
-  if ((e = cudaFuncSetAttribute(colpass_kernel_b<N, 2, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps))) return e;
-  if constexpr (RCfg<N, T>::ON) {
+  if constexpr (!RCfg<N, T>::ON) {
+    const int ps = (int)colsmem<N, T>();
+    if ((e = cudaFuncSetAttribute(colpass_kernel<N, 0, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps))) return e;
+    if ((e = cudaFuncSetAttribute(colpass_kernel<N, 1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps))) return e;
+    if ((e = cudaFuncSetAttribute(colpass_kernel<N, 2, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps))) return e;
+    if ((e = cudaFuncSetAttribute(colpass_kernel_b<N, 0, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps))) return e;
+    if ((e = cudaFuncSetAttribute(colpass_kernel_b<N, 1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps))) return e;
+    if ((e = cudaFuncSetAttribute(colpass_kernel_b<N, 2, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps))) return e;
+  } else {
     const int rs = (int)rcolsmem<N, T>();
     if ((e = cudaFuncSetAttribute(rcol_kernel<N, 0, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, rs))) return e;
     if ((e = cudaFuncSetAttribute(rcol_kernel<N, 1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, rs))) return e;
@@ -592,13 +772,13 @@ static void launch_xfwd(const PoissonArgs<T>& a, cudaStream_t st) {
   const dim3 gx(N / (2 * G::P), N);
   const size_t xs = xsmem<N, T>();
   if (a.rhs)
-    xfwd_kernel<N, 1, T><<<gx, G::NT, xs, st>>>(nullptr, nullptr, nullptr, a.rhs, nullptr, a.spec, a.tw, a.ctrl,
+    xfwd_kernel<N, 1, T><<<gx, XCfg<N, T>::NT, xs, st>>>(nullptr, nullptr, nullptr, a.rhs, nullptr, a.spec, a.tw, a.ctrl,
                                                 a.cdiv, a.ddxi);
   else if (a.pres)
-    xfwd_kernel<N, 2, T><<<gx, G::NT, xs, st>>>(a.us, a.vs, a.ws, nullptr, a.pres, a.spec, a.tw, a.ctrl, a.cdiv,
+    xfwd_kernel<N, 2, T><<<gx, XCfg<N, T>::NT, xs, st>>>(a.us, a.vs, a.ws, nullptr, a.pres, a.spec, a.tw, a.ctrl, a.cdiv,
                                                 a.ddxi);
   else
-    xfwd_kernel<N, 0, T><<<gx, G::NT, xs, st>>>(a.us, a.vs, a.ws, nullptr, nullptr, a.spec, a.tw, a.ctrl, a.cdiv,
+    xfwd_kernel<N, 0, T><<<gx, XCfg<N, T>::NT, xs, st>>>(a.us, a.vs, a.ws, nullptr, nullptr, a.spec, a.tw, a.ctrl, a.cdiv,
                                                 a.ddxi);
 }
 
@@ -611,7 +791,7 @@ static cudaError_t poisson_run(const PoissonArgs<T>& a, cudaStream_t st) {
   launch_col<N, 0, T>(a, st);
   launch_col<N, 2, T>(a, st);
   launch_col<N, 1, T>(a, st);
-  xinv_kernel<N, T><<<gx, G::NT, xs, st>>>(a.spec, a.p, a.tw, a.ctrl);
+  xinv_kernel<N, T><<<gx, XCfg<N, T>::NT, xs, st>>>(a.spec, a.p, a.tw, a.ctrl);
   return cudaGetLastError();
 }
 
@@ -625,7 +805,7 @@ static cudaError_t poisson_stage(const PoissonArgs<T>& a, int stage, cudaStream_
     case 1: launch_col<N, 0, T>(a, st); break;
     case 2: launch_col<N, 2, T>(a, st); break;
     case 3: launch_col<N, 1, T>(a, st); break;
-    case 4: xinv_kernel<N, T><<<gx, G::NT, xs, st>>>(a.spec, a.p, a.tw, a.ctrl); break;
+    case 4: xinv_kernel<N, T><<<gx, XCfg<N, T>::NT, xs, st>>>(a.spec, a.p, a.tw, a.ctrl); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
@@ -654,14 +834,14 @@ static cudaError_t poisson_stage_b(const SlotArgs<T>* slots, int nslots, int sta
   switch (stage) {
     case 0:
       if (which)
-        xfwd_kernel_b<N, 2, T><<<gx, G::NT, xs, st>>>(slots, 1);
+        xfwd_kernel_b<N, 2, T><<<gx, XCfg<N, T>::NT, xs, st>>>(slots, 1);
       else
-        xfwd_kernel_b<N, 0, T><<<gx, G::NT, xs, st>>>(slots, 0);
+        xfwd_kernel_b<N, 0, T><<<gx, XCfg<N, T>::NT, xs, st>>>(slots, 0);
       break;
     case 1: launch_col_b<N, 0, T>(slots, nslots, which, st); break;
     case 2: launch_col_b<N, 2, T>(slots, nslots, which, st); break;
     case 3: launch_col_b<N, 1, T>(slots, nslots, which, st); break;
-    case 4: xinv_kernel_b<N, T><<<gx, G::NT, xs, st>>>(slots, which); break;
+    case 4: xinv_kernel_b<N, T><<<gx, XCfg<N, T>::NT, xs, st>>>(slots, which); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
