@@ -171,12 +171,22 @@ template <int N, int NS, int L, int NT, int DIR, class C> struct FFTRun {
 // same order, so both transforms give the same bits.
 //
 // Exchange buffer: `at(n)` is the shared-memory slot of element n of the
-// thread's line.  Both layouts in use pad one element after every 8
-// (n + n/8), which keeps a stage's stride-R writes free of bank conflicts:
-// lines interleaved (element n of line c at (n + n/8)*CC + c, for column
-// slabs whose rows are narrower than 128 bytes) or one line after another
-// (line c at c*reg_rows(N) + n + n/8, for x lines).
+// thread's line.  The exchanges write either consecutive elements or
+// elements 8 apart (d = 8j + r over consecutive j), and both must be free of
+// bank conflicts for the phase a warp's access is split into (8 lanes for
+// 16-byte elements, 16 for 8-byte ones).  Two index maps do that:
+//   * reg_pad: one pad element after every 8 (n + n/8).  Lines are
+//     interleaved for column slabs (element n of line c at pad(n)*CC + c)
+//     and follow one another for FP64 x lines (c*reg_rows(N) + pad(n)).
+//   * reg_swz: an XOR swizzle within aligned groups of 16, n ^ ((n/8) & 15),
+//     for FP32 x lines (c*N + swz(n)).  With 8-byte elements a phase reads
+//     16 consecutive elements, which the pad map splits unevenly over the
+//     banks; the swizzle keeps them distinct (512^3: FP32 x inverse
+//     0.28 -> 0.25 ms), while for FP64 its extra index arithmetic costs more
+//     than it saves.
 __host__ __device__ constexpr int reg_rows(int N) { return N + N / 8; }
+__device__ __forceinline__ int reg_pad(int n) { return n + (n >> 3); }
+__device__ __forceinline__ int reg_swz(int n) { return n ^ ((n >> 3) & 15); }
 
 template <int N, int NS, int DIR, class C, class At>
 __device__ __forceinline__ void reg_fft_stages(C (&v)[8], C* s, const C* __restrict__ tw, int t, const At& at) {

@@ -334,7 +334,7 @@ __device__ __forceinline__ void rcol_run(int total, const typename C2<T>::t* __r
     tw = stw;
   }
   const int c = threadIdx.x % CC, t = threadIdx.x / CC;
-  const auto at = [c](int n) { return (n + (n >> 3)) * CC + c; };
+  const auto at = [c](int n) { return reg_pad(n) * CC + c; };
   // prefetch: each thread copies its own eight elements of the next slab into
   // its own slots (m*NT + tid), so only its own cp.async wait orders them
   auto prefetch = [&](const ColSlab& ps) {
@@ -526,6 +526,9 @@ __device__ __forceinline__ void xinv_body(const typename C2<T>::t* __restrict__ 
 template <int N, class T> struct XCfg {
   static constexpr bool ON = RCfg<N, T>::ON;
   static constexpr int NT = ON ? PCfg<N, T>::P * (N / 8) : PCfg<N, T>::NT;
+  // exchange slots of a line (see reg_pad / reg_swz) and the line stride
+  static constexpr int LS = sizeof(T) == 8 ? reg_rows(N) : N;
+  static __device__ __forceinline__ int slot(int n) { return sizeof(T) == 8 ? reg_pad(n) : reg_swz(n); }
 };
 
 template <int N, class T>
@@ -534,7 +537,7 @@ __device__ __forceinline__ void xinv_reg_body(const typename C2<T>::t* __restric
                                               const Ctrl* __restrict__ ctrl, int bx, int by) {
   typedef typename C2<T>::t C;
   typedef PCfg<N, T> G;
-  constexpr int TPC = N / 8, RS = reg_rows(N);
+  constexpr int TPC = N / 8;
   if (ctrl && ctrl->status) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* s = reinterpret_cast<C*>(smem_raw);
@@ -568,8 +571,8 @@ __device__ __forceinline__ void xinv_reg_body(const typename C2<T>::t* __restric
       v[m].y = b.x - a.y;
     }
   }
-  const int base = q * RS;
-  reg_fft_stages<N, 1, +1>(v, s, tw, t, [base](int n) { return base + n + (n >> 3); });
+  const int base = q * XCfg<N, T>::LS;
+  reg_fft_stages<N, 1, +1>(v, s, tw, t, [base](int n) { return base + XCfg<N, T>::slot(n); });
 #pragma unroll
   for (int m = 0; m < 8; ++m) {
     const int n = t + TPC * m;
@@ -587,7 +590,7 @@ __device__ __forceinline__ void xfwd_reg_body(const T* __restrict__ us, const T*
                                               int by) {
   typedef typename C2<T>::t C;
   typedef PCfg<N, T> G;
-  constexpr int TPC = N / 8, RS = reg_rows(N), M = N / 2 + 1;
+  constexpr int TPC = N / 8, M = N / 2 + 1;
   if (ctrl && ctrl->status) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* s = reinterpret_cast<C*>(smem_raw);
@@ -601,8 +604,8 @@ __device__ __forceinline__ void xfwd_reg_body(const T* __restrict__ us, const T*
     v[m].x = (T)xfwd_rhs<N, MODE, T>(us, vs, ws, rhs, p0, cdiv, ddxi, n, ja, k);
     v[m].y = (T)xfwd_rhs<N, MODE, T>(us, vs, ws, rhs, p0, cdiv, ddxi, n, ja + 1, k);
   }
-  const int base = q * RS;
-  const auto at = [base](int n) { return base + n + (n >> 3); };
+  const int base = q * XCfg<N, T>::LS;
+  const auto at = [base](int n) { return base + XCfg<N, T>::slot(n); };
   reg_fft_stages<N, 1, -1>(v, s, tw, t, at);
 #pragma unroll
   for (int m = 0; m < 8; ++m) s[at(t + TPC * m)] = v[m];
@@ -611,9 +614,9 @@ __device__ __forceinline__ void xfwd_reg_body(const T* __restrict__ us, const T*
   for (int wi = threadIdx.x; wi < G::P * M; wi += XCfg<N, T>::NT) {
     const int m = wi % M, pq = wi / M;
     const int jb = j0 + 2 * pq;
-    const C zm = s[pq * RS + m + (m >> 3)];
+    const C zm = s[pq * XCfg<N, T>::LS + XCfg<N, T>::slot(m)];
     const int mr = (m == 0) ? 0 : (N - m);
-    const C zr = s[pq * RS + mr + (mr >> 3)];
+    const C zr = s[pq * XCfg<N, T>::LS + XCfg<N, T>::slot(mr)];
     C Am, Bm;
     Am.x = half * (zm.x + zr.x);
     Am.y = half * (zm.y - zr.y);
@@ -675,7 +678,7 @@ __global__ void __launch_bounds__(256, 3) xinv_kernel_b(const SlotArgs<T>* __res
 
 // ---------------------------------------------------------------- launchers
 template <int N, class T> static size_t xsmem() {
-  if constexpr (XCfg<N, T>::ON) return (size_t)PCfg<N, T>::P * reg_rows(N) * sizeof(typename C2<T>::t);
+  if constexpr (XCfg<N, T>::ON) return (size_t)PCfg<N, T>::P * XCfg<N, T>::LS * sizeof(typename C2<T>::t);
   return (size_t)N * Pitch<PCfg<N, T>::P>::value * sizeof(typename C2<T>::t);
 }
 
