@@ -173,7 +173,7 @@ std::vector<Stage> step_stages(mhit_handle* h, int cur) {
   std::vector<Stage> v;
   cudaStream_t st = h->st;
   const int n = h->n;
-  const int kz = h->kz, mty = h->mty ? h->mty : mhit::default_mty(n);
+  const int kz = h->kz, mty = h->mty ? h->mty : mhit::default_mty(n, h->precision != MHIT_FP64);
   const bool pf = h->phase_field != 0;
   static const char* pnames[5] = {"xfwd", "yfwd", "zsolve", "yinv", "xinv"};
   static const char* rnames[5] = {"xres", "yfwd2", "zsolve2", "yinv2", "xinv2"};

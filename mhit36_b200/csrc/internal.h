@@ -85,7 +85,7 @@ int stencil_kz_ok(int n, int kz);
 template <class T> cudaError_t launch_phase(const StencilArgs<T>& a, cudaStream_t st, int kz);
 template <class T>
 cudaError_t launch_momentum(const StencilArgs<T>& a, bool phase_field, cudaStream_t st, int kz, int mty);
-int default_mty(int n);
+int default_mty(int n, int fp32);
 template <class T> cudaError_t launch_project(const StencilArgs<T>& a, cudaStream_t st);
 // FP32 refinement form: p = p0 + dp, projection and max|div u| in FP64.
 cudaError_t launch_project_refine(const StencilArgs<float>& a, const float* dp, cudaStream_t st);

@@ -28,9 +28,10 @@ constexpr int TX = 32, TY = 8, NT = TX * TY;
 // below, so that smaller grids keep enough CTAs.
 static int pick_kz(int n) { return n >= 512 ? 64 : (n >= 32 ? 32 : n); }
 
-// Momentum tile height (measured on B200 at 256^3 and 512^3 with the
-// one-plane cp.async prefetch: 8 rows beat 16 by 20% at both sizes).
-int default_mty(int n) { return n > 0 ? 8 : 8; }
+// Momentum tile height.  Both tiles run 256 threads; the 16-row tile gives
+// each thread two rows.  Measured on B200 at 512^3: FP64 8 rows 3.06 ms,
+// 16 rows 4.18 ms (128 registers); FP32 8 rows 2.00 ms, 16 rows 1.87 ms.
+int default_mty(int n, int fp32) { return (n >= 16 && fp32) ? 16 : 8; }
 
 // ============================================================ phase field
 // ACDI step A1..A7 (multi/main.f90:341-480) fused into one kernel:
@@ -41,8 +42,13 @@ int default_mty(int n) { return n > 0 ? 8 : 8; }
 //   phi_new = phi + dt*rhs                                    (A7)
 // psi needs phi on a radius-2 neighbourhood; it is computed per plane on the
 // tile plus a 2-cell ring, F on the tile plus a 1-cell ring.
+// Tile 32 x 16 with two output rows per thread (rows ty and ty + 8, 256
+// threads): the per-plane barriers, ring bookkeeping and copy issue are
+// shared by two points, and the psi / F loops run three rounds per thread
+// (B200, 512^3 FP64: 2.61 -> 2.36 ms against one row per thread).
 constexpr int PTY = 16;            // phase tile height
-constexpr int PNT = TX * PTY;       // phase threads per CTA
+constexpr int PPT = 2;             // output rows per thread (rows ty + h*PTY/PPT)
+constexpr int PNT = TX * PTY / PPT;  // phase threads per CTA
 
 // Momentum ring depth (planes per field): planes m-2 .. m+1, one in flight.
 // (A 5-plane ring with two planes in flight measured 30% slower on B200 at
@@ -92,8 +98,9 @@ __device__ __forceinline__ void phase_body(const StencilArgs<T>& a, int KZ, int 
   const T psi1 = eps * log(((T)1 + enumv) / ((T)1 - (T)1 + enumv));
   const int x0 = bx * TX, y0 = by * TY, k0 = bz * KZ;
   const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
-  const int i = x0 + tx, j = y0 + ty;
-  const int ip = (i + 1 == n) ? 0 : i + 1, jp = (j + 1 == n) ? 0 : j + 1;
+  constexpr int RY = TY / PPT;  // row step between a thread's output rows
+  const int i = x0 + tx;
+  const int ip = (i + 1 == n) ? 0 : i + 1;
   const size_t nn = (size_t)n * n;
   // Each thread owns ring elements tid + r*NT of every plane (copy and psi)
   // and F elements tid + r*NT; their in-plane offsets are the same on every
@@ -117,7 +124,14 @@ __device__ __forceinline__ void phase_body(const StencilArgs<T>& a, int KZ, int 
   T *Phm3 = s_phi, *Phm2 = s_phi + PE, *Phm1 = s_phi + 2 * PE, *Ph0 = s_phi + 3 * PE, *Php1 = s_phi + 4 * PE;
   T *PsW = s_psi, *Psm1 = s_psi + PE, *Psm2 = s_psi + 2 * PE;
   T *FW = s_F, *Fm2 = s_F + 3 * FE, *Fm3 = s_F + 6 * FE;
-  const int gij = i + n * j, gipj = ip + n * j, gijp = i + n * jp;
+  int gij[PPT], gipj[PPT], gijp[PPT];
+#pragma unroll
+  for (int h = 0; h < PPT; ++h) {
+    const int j = y0 + ty + h * RY, jp = (j + 1 == n) ? 0 : j + 1;
+    gij[h] = i + n * j;
+    gipj[h] = ip + n * j;
+    gijp[h] = i + n * jp;
+  }
 
   // phi plane m (2-cell ring) is copied into `dst` with cp.async one
   // iteration ahead of its use.
@@ -138,15 +152,18 @@ __device__ __forceinline__ void phase_body(const StencilArgs<T>& a, int KZ, int 
     cp_async_wait<1>();  // this thread's copies of plane m have landed
     // velocities of the output plane k = m-2, loaded now so that their latency
     // hides behind the psi and F work below
-    T uc = 0, uxp = 0, vc = 0, vyp = 0, wc = 0, wzp = 0;
+    T uc[PPT], uxp[PPT], vc[PPT], vyp[PPT], wc[PPT], wzp[PPT];
     if (m >= k0 + 2) {
       const size_t zo = nn * wrapi(m - 2, n), zop = nn * wrapi(m - 1, n);
-      uc = a.u[zo + gij];
-      uxp = a.u[zo + gipj];
-      vc = a.v[zo + gij];
-      vyp = a.v[zo + gijp];
-      wc = a.w[zo + gij];
-      wzp = a.w[zop + gij];
+#pragma unroll
+      for (int h = 0; h < PPT; ++h) {
+        uc[h] = a.u[zo + gij[h]];
+        uxp[h] = a.u[zo + gipj[h]];
+        vc[h] = a.v[zo + gij[h]];
+        vyp[h] = a.v[zo + gijp[h]];
+        wc[h] = a.w[zo + gij[h]];
+        wzp[h] = a.w[zop + gij[h]];
+      }
     }
     // (1) psi of plane m on the elements this thread copied.
 #pragma unroll
@@ -204,22 +221,26 @@ __device__ __forceinline__ void phase_body(const StencilArgs<T>& a, int KZ, int 
       const T* F0 = Fm2;
       const T* Fm = Fm3;
       const T* Fp = FW;
-      const int pe = (tx + 2) + (ty + 2) * EX;
-      const int fe = (tx + 1) + (ty + 1) * FX;
-      const T c = P0[pe], pxp = P0[pe + 1], pxm = P0[pe - 1], pyp = P0[pe + EX], pym = P0[pe - EX];
-      const T pzp = Pp1[pe], pzm = Pm1[pe];
-      const size_t g = nn * wrapi(m - 2, n) + gij;
-      uc -= mu; uxp -= mu; vc -= mv; vyp -= mv; wc -= mw; wzp -= mw;
-      // The factors 0.5 of the face averages and central differences are
-      // folded into hdxi = 0.5*dxi: scaling by a power of 2 commutes with
-      // rounding, so every term is bitwise the reference's (x*0.5*y - ..)*dxi.
-      T r = -(uxp * (pxp + c) - uc * (c + pxm)) * hdxi - (vyp * (pyp + c) - vc * (c + pym)) * hdxi -
-            (wzp * (pzp + c) - wc * (c + pzm)) * hdxi;
-      r = r + gamma * (eps * (pxp - (T)2 * c + pxm) * ddxi + eps * (pyp - (T)2 * c + pym) * ddxi +
-                       eps * (pzp - (T)2 * c + pzm) * ddxi);
-      r = r - gamma * ((F0[fe + 1] - F0[fe - 1]) * hdxi + (F0[FE + fe + FX] - F0[FE + fe - FX]) * hdxi +
-                       (Fp[2 * FE + fe] - Fm[2 * FE + fe]) * hdxi);
-      a.phi_out[g] = c + dt * r;
+#pragma unroll
+      for (int h = 0; h < PPT; ++h) {
+        const int pe = (tx + 2) + (ty + h * RY + 2) * EX;
+        const int fe = (tx + 1) + (ty + h * RY + 1) * FX;
+        const T c = P0[pe], pxp = P0[pe + 1], pxm = P0[pe - 1], pyp = P0[pe + EX], pym = P0[pe - EX];
+        const T pzp = Pp1[pe], pzm = Pm1[pe];
+        const size_t g = nn * wrapi(m - 2, n) + gij[h];
+        const T uc_ = uc[h] - mu, uxp_ = uxp[h] - mu, vc_ = vc[h] - mv, vyp_ = vyp[h] - mv;
+        const T wc_ = wc[h] - mw, wzp_ = wzp[h] - mw;
+        // The factors 0.5 of the face averages and central differences are
+        // folded into hdxi = 0.5*dxi: scaling by a power of 2 commutes with
+        // rounding, so every term is bitwise the reference's (x*0.5*y - ..)*dxi.
+        T r = -(uxp_ * (pxp + c) - uc_ * (c + pxm)) * hdxi - (vyp_ * (pyp + c) - vc_ * (c + pym)) * hdxi -
+              (wzp_ * (pzp + c) - wc_ * (c + pzm)) * hdxi;
+        r = r + gamma * (eps * (pxp - (T)2 * c + pxm) * ddxi + eps * (pyp - (T)2 * c + pym) * ddxi +
+                         eps * (pzp - (T)2 * c + pzm) * ddxi);
+        r = r - gamma * ((F0[fe + 1] - F0[fe - 1]) * hdxi + (F0[FE + fe + FX] - F0[FE + fe - FX]) * hdxi +
+                         (Fp[2 * FE + fe] - Fm[2 * FE + fe]) * hdxi);
+        a.phi_out[g] = c + dt * r;
+      }
     }
     // rotate the rings for plane m+1: the slot of the oldest plane of each
     // ring takes the next plane
@@ -242,7 +263,8 @@ __device__ __forceinline__ void phase_body(const StencilArgs<T>& a, int KZ, int 
 template <class T, bool PF, int MTYv>
 __device__ __forceinline__ void momentum_body(const StencilArgs<T>& a, int KZ, int bx, int by, int bz) {
   if (a.ctrl->status) return;
-  constexpr int TY = MTYv, NT = TX * MTYv;
+  // MPT output rows per thread (rows ty + 8h): 256 threads for either tile
+  constexpr int TY = MTYv, MPT = MTYv / 8, NT = TX * 8;
   constexpr int UX = TX + 2, UY = TY + 2, UE = UX * UY;  // velocity planes, 1-cell ring
   constexpr int EX = TX + 4, EY = TY + 4, PE = EX * EY;  // phi planes, 2-cell ring
   constexpr int QX = TX + 1, QY = TY + 1, QE = QX * QY;  // force over [-1,TX) x [-1,TY)
@@ -263,7 +285,7 @@ __device__ __forceinline__ void momentum_body(const StencilArgs<T>& a, int KZ, i
   const T mu = (T)a.ctrl->mean[0], mv = (T)a.ctrl->mean[1], mw = (T)a.ctrl->mean[2];
   const int x0 = bx * TX, y0 = by * TY, k0 = bz * KZ;
   const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
-  const int i = x0 + tx, j = y0 + ty;
+  const int i = x0 + tx;
   const size_t nn = (size_t)n * n;
   const T h = (T)0.5, q = (T)0.25;
   const T qdxi = q * dxi, hrhoi = h * rhoi;
@@ -322,7 +344,8 @@ __device__ __forceinline__ void momentum_body(const StencilArgs<T>& a, int KZ, i
 #pragma unroll
   for (int q2 = 0; q2 < PD; ++q2) issue(sl[2 + q2], k0 - 2 + q2);
   // registers carried from one output plane to the next (see below)
-  T r_uc = 0, r_uzp = 0, r_uxp = 0, r_vc = 0, r_vzp = 0, r_vyp = 0, r_wc = 0, r_wzp = 0, r_wxmzp = 0, r_wymzp = 0;
+  T r_uc[MPT], r_uzp[MPT], r_uxp[MPT], r_vc[MPT], r_vzp[MPT], r_vyp[MPT], r_wc[MPT], r_wzp[MPT], r_wxmzp[MPT],
+      r_wymzp[MPT];
   bool have_prev = false;
   for (int m = k0 - 2; m <= k0 + KZ; ++m) {
     __syncthreads();  // every thread is done with the slot plane m+PD reuses
@@ -331,12 +354,15 @@ __device__ __forceinline__ void momentum_body(const StencilArgs<T>& a, int KZ, i
     cp_async_wait<PD>();  // this thread's copies of plane m have landed
     // rhs_o of the output plane k = m-1, loaded now so that its latency hides
     // behind the force computation below
-    T ruo = 0, rvo = 0, rwo = 0;
+    T ruo[MPT], rvo[MPT], rwo[MPT];
     if (m >= k0 + 1) {
-      const size_t g = (size_t)i + (size_t)n * j + nn * wrapi(m - 1, n);
-      ruo = a.ru[g];
-      rvo = a.rv[g];
-      rwo = a.rw[g];
+#pragma unroll
+      for (int hh = 0; hh < MPT; ++hh) {
+        const size_t g = (size_t)i + (size_t)n * (y0 + ty + 8 * hh) + nn * wrapi(m - 1, n);
+        ruo[hh] = a.ru[g];
+        rvo[hh] = a.rv[g];
+        rwo[hh] = a.rw[g];
+      }
     }
     __syncthreads();
     if (PF && m >= k0) {
@@ -373,90 +399,94 @@ __device__ __forceinline__ void momentum_body(const StencilArgs<T>& a, int KZ, i
       const T* W0 = s_w + sl[1] * UE;
       const T* Wm = s_w + sl[0] * UE;
       const T* Wp = s_w + sl[2] * UE;
-      const int e = (tx + 1) + (ty + 1) * UX;
-      // The pending mean removal is applied as values enter registers.  Values
-      // of this thread's column at planes k-1 and k, and the x/y neighbours
-      // the previous plane already loaded, come from the previous output
-      // plane's registers (z-marching register blocking): 17 shared loads
-      // per point instead of 27.
-      T uc, uzm, uxpzm, vc, vzm, vypzm, wc, wzm, wxm, wym;
-      if (have_prev) {
-        uzm = r_uc; uc = r_uzp; uxpzm = r_uxp;
-        vzm = r_vc; vc = r_vzp; vypzm = r_vyp;
-        wzm = r_wc; wc = r_wzp; wxm = r_wxmzp; wym = r_wymzp;
-      } else {
-        uc = U0[e] - mu; uzm = Um[e] - mu; uxpzm = Um[e + 1] - mu;
-        vc = V0[e] - mv; vzm = Vm[e] - mv; vypzm = Vm[e + UX] - mv;
-        wc = W0[e] - mw; wzm = Wm[e] - mw; wxm = W0[e - 1] - mw; wym = W0[e - UX] - mw;
+#pragma unroll
+      for (int hh = 0; hh < MPT; ++hh) {
+        const int j = y0 + ty + 8 * hh;
+        const int e = (tx + 1) + (ty + 8 * hh + 1) * UX;
+        // The pending mean removal is applied as values enter registers.  Values
+        // of this thread's column at planes k-1 and k, and the x/y neighbours
+        // the previous plane already loaded, come from the previous output
+        // plane's registers (z-marching register blocking): 17 shared loads
+        // per point instead of 27.
+        T uc, uzm, uxpzm, vc, vzm, vypzm, wc, wzm, wxm, wym;
+        if (have_prev) {
+          uzm = r_uc[hh]; uc = r_uzp[hh]; uxpzm = r_uxp[hh];
+          vzm = r_vc[hh]; vc = r_vzp[hh]; vypzm = r_vyp[hh];
+          wzm = r_wc[hh]; wc = r_wzp[hh]; wxm = r_wxmzp[hh]; wym = r_wymzp[hh];
+        } else {
+          uc = U0[e] - mu; uzm = Um[e] - mu; uxpzm = Um[e + 1] - mu;
+          vc = V0[e] - mv; vzm = Vm[e] - mv; vypzm = Vm[e + UX] - mv;
+          wc = W0[e] - mw; wzm = Wm[e] - mw; wxm = W0[e - 1] - mw; wym = W0[e - UX] - mw;
+        }
+        const T uxp = U0[e + 1] - mu, uxm = U0[e - 1] - mu, uyp = U0[e + UX] - mu, uym = U0[e - UX] - mu;
+        const T uzp = Up[e] - mu, uxpym = U0[e + 1 - UX] - mu;
+        const T vxp = V0[e + 1] - mv, vxm = V0[e - 1] - mv, vyp = V0[e + UX] - mv, vym = V0[e - UX] - mv;
+        const T vzp = Vp[e] - mv, vxmyp = V0[e - 1 + UX] - mv;
+        const T wxp = W0[e + 1] - mw, wyp = W0[e + UX] - mw;
+        const T wzp = Wp[e] - mw, wxmzp = Wp[e - 1] - mw, wymzp = Wp[e - UX] - mw;
+        r_uc[hh] = uc; r_uzp[hh] = uzp; r_uxp[hh] = uxp;
+        r_vc[hh] = vc; r_vzp[hh] = vzp; r_vyp[hh] = vyp;
+        r_wc[hh] = wc; r_wzp[hh] = wzp; r_wxmzp[hh] = wxmzp; r_wymzp[hh] = wymzp;
+        // B1 (multi/main.f90:527-549)
+        T h11 = (uxp + uc) * (uxp + uc) - (uc + uxm) * (uc + uxm);
+        T h12 = (uyp + uc) * (vyp + vxmyp) - (uc + uym) * (vc + vxm);
+        T h13 = (uzp + uc) * (wzp + wxmzp) - (uc + uzm) * (wc + wxm);
+        T h21 = (uxp + uxpym) * (vxp + vc) - (uc + uym) * (vc + vxm);
+        T h22 = (vyp + vc) * (vyp + vc) - (vc + vym) * (vc + vym);
+        T h23 = (wzp + wymzp) * (vzp + vc) - (wc + wym) * (vc + vzm);
+        T h31 = (wxp + wc) * (uxp + uxpzm) - (wc + wxm) * (uc + uzm);
+        T h32 = (vyp + vypzm) * (wyp + wc) - (vc + vzm) * (wc + wym);
+        T h33 = (wzp + wc) * (wzp + wc) - (wc + wzm) * (wc + wzm);
+        // (h * 0.25) * dxi == h * (0.25 * dxi) exactly: scaling by a power of 2
+        h11 = h11 * qdxi; h12 = h12 * qdxi; h13 = h13 * qdxi;
+        h21 = h21 * qdxi; h22 = h22 * qdxi; h23 = h23 * qdxi;
+        h31 = h31 * qdxi; h32 = h32 * qdxi; h33 = h33 * qdxi;
+        T ru = -(h11 + h12 + h13);
+        T rv = -(h21 + h22 + h23);
+        T rw = -(h31 + h32 + h33);
+        // B2 (multi/main.f90:567-578)
+        h11 = mu_v * (uxp - (T)2 * uc + uxm) * ddxi;
+        h12 = mu_v * (uyp - (T)2 * uc + uym) * ddxi;
+        h13 = mu_v * (uzp - (T)2 * uc + uzm) * ddxi;
+        h21 = mu_v * (vxp - (T)2 * vc + vxm) * ddxi;
+        h22 = mu_v * (vyp - (T)2 * vc + vym) * ddxi;
+        h23 = mu_v * (vzp - (T)2 * vc + vzm) * ddxi;
+        h31 = mu_v * (wxp - (T)2 * wc + wxm) * ddxi;
+        h32 = mu_v * (wyp - (T)2 * wc + wym) * ddxi;
+        h33 = mu_v * (wzp - (T)2 * wc + wzm) * ddxi;
+        ru = ru + (h11 + h12 + h13) * rhoi;
+        rv = rv + (h21 + h22 + h23) * rhoi;
+        rw = rw + (h31 + h32 + h33) * rhoi;
+        const int kz = wrapi(k, n);
+        // B3 ABC forcing (multi/main.f90:591-593), global interior coordinates
+        if (a.c.abc) {
+          ru = ru + f3 * (T)a.fsin[kz] + f2 * (T)a.fcos[j];
+          rv = rv + f1 * (T)a.fsin[i] + f3 * (T)a.fcos[kz];
+          rw = rw + f2 * (T)a.fsin[j] + f1 * (T)a.fcos[i];
+        }
+        if (lin != (T)0) {  // linear forcing (extension)
+          ru = ru + lin * uc;
+          rv = rv + lin * vc;
+          rw = rw + lin * wc;
+        }
+        if (PF) {  // B5 (multi/main.f90:652-654)
+          const T* F0 = s_f + ((k + 8) & 1) * 3 * QE;
+          const T* Fm = s_f + ((k + 7) & 1) * 3 * QE;
+          const int qe = (tx + 1) + (ty + 8 * hh + 1) * QX;
+          ru = ru + (F0[qe - 1] + F0[qe]) * hrhoi;  // == 0.5 * (..) * rhoi exactly
+          rv = rv + (F0[QE + qe - QX] + F0[QE + qe]) * hrhoi;
+          rw = rw + (Fm[2 * QE + qe] + F0[2 * QE + qe]) * hrhoi;
+        }
+        // B6, B7 (multi/main.f90:666-681)
+        const size_t g = (size_t)i + (size_t)n * j + nn * kz;
+        a.us[g] = uc + dt * (alpha * ru - beta * ruo[hh]);
+        a.vs[g] = vc + dt * (alpha * rv - beta * rvo[hh]);
+        a.ws[g] = wc + dt * (alpha * rw - beta * rwo[hh]);
+        a.ru[g] = ru;
+        a.rv[g] = rv;
+        a.rw[g] = rw;
       }
-      const T uxp = U0[e + 1] - mu, uxm = U0[e - 1] - mu, uyp = U0[e + UX] - mu, uym = U0[e - UX] - mu;
-      const T uzp = Up[e] - mu, uxpym = U0[e + 1 - UX] - mu;
-      const T vxp = V0[e + 1] - mv, vxm = V0[e - 1] - mv, vyp = V0[e + UX] - mv, vym = V0[e - UX] - mv;
-      const T vzp = Vp[e] - mv, vxmyp = V0[e - 1 + UX] - mv;
-      const T wxp = W0[e + 1] - mw, wyp = W0[e + UX] - mw;
-      const T wzp = Wp[e] - mw, wxmzp = Wp[e - 1] - mw, wymzp = Wp[e - UX] - mw;
-      r_uc = uc; r_uzp = uzp; r_uxp = uxp;
-      r_vc = vc; r_vzp = vzp; r_vyp = vyp;
-      r_wc = wc; r_wzp = wzp; r_wxmzp = wxmzp; r_wymzp = wymzp;
       have_prev = true;
-      // B1 (multi/main.f90:527-549)
-      T h11 = (uxp + uc) * (uxp + uc) - (uc + uxm) * (uc + uxm);
-      T h12 = (uyp + uc) * (vyp + vxmyp) - (uc + uym) * (vc + vxm);
-      T h13 = (uzp + uc) * (wzp + wxmzp) - (uc + uzm) * (wc + wxm);
-      T h21 = (uxp + uxpym) * (vxp + vc) - (uc + uym) * (vc + vxm);
-      T h22 = (vyp + vc) * (vyp + vc) - (vc + vym) * (vc + vym);
-      T h23 = (wzp + wymzp) * (vzp + vc) - (wc + wym) * (vc + vzm);
-      T h31 = (wxp + wc) * (uxp + uxpzm) - (wc + wxm) * (uc + uzm);
-      T h32 = (vyp + vypzm) * (wyp + wc) - (vc + vzm) * (wc + wym);
-      T h33 = (wzp + wc) * (wzp + wc) - (wc + wzm) * (wc + wzm);
-      // (h * 0.25) * dxi == h * (0.25 * dxi) exactly: scaling by a power of 2
-      h11 = h11 * qdxi; h12 = h12 * qdxi; h13 = h13 * qdxi;
-      h21 = h21 * qdxi; h22 = h22 * qdxi; h23 = h23 * qdxi;
-      h31 = h31 * qdxi; h32 = h32 * qdxi; h33 = h33 * qdxi;
-      T ru = -(h11 + h12 + h13);
-      T rv = -(h21 + h22 + h23);
-      T rw = -(h31 + h32 + h33);
-      // B2 (multi/main.f90:567-578)
-      h11 = mu_v * (uxp - (T)2 * uc + uxm) * ddxi;
-      h12 = mu_v * (uyp - (T)2 * uc + uym) * ddxi;
-      h13 = mu_v * (uzp - (T)2 * uc + uzm) * ddxi;
-      h21 = mu_v * (vxp - (T)2 * vc + vxm) * ddxi;
-      h22 = mu_v * (vyp - (T)2 * vc + vym) * ddxi;
-      h23 = mu_v * (vzp - (T)2 * vc + vzm) * ddxi;
-      h31 = mu_v * (wxp - (T)2 * wc + wxm) * ddxi;
-      h32 = mu_v * (wyp - (T)2 * wc + wym) * ddxi;
-      h33 = mu_v * (wzp - (T)2 * wc + wzm) * ddxi;
-      ru = ru + (h11 + h12 + h13) * rhoi;
-      rv = rv + (h21 + h22 + h23) * rhoi;
-      rw = rw + (h31 + h32 + h33) * rhoi;
-      const int kz = wrapi(k, n);
-      // B3 ABC forcing (multi/main.f90:591-593), global interior coordinates
-      if (a.c.abc) {
-        ru = ru + f3 * (T)a.fsin[kz] + f2 * (T)a.fcos[j];
-        rv = rv + f1 * (T)a.fsin[i] + f3 * (T)a.fcos[kz];
-        rw = rw + f2 * (T)a.fsin[j] + f1 * (T)a.fcos[i];
-      }
-      if (lin != (T)0) {  // linear forcing (extension)
-        ru = ru + lin * uc;
-        rv = rv + lin * vc;
-        rw = rw + lin * wc;
-      }
-      if (PF) {  // B5 (multi/main.f90:652-654)
-        const T* F0 = s_f + ((k + 8) & 1) * 3 * QE;
-        const T* Fm = s_f + ((k + 7) & 1) * 3 * QE;
-        const int qe = (tx + 1) + (ty + 1) * QX;
-        ru = ru + (F0[qe - 1] + F0[qe]) * hrhoi;  // == 0.5 * (..) * rhoi exactly
-        rv = rv + (F0[QE + qe - QX] + F0[QE + qe]) * hrhoi;
-        rw = rw + (Fm[2 * QE + qe] + F0[2 * QE + qe]) * hrhoi;
-      }
-      // B6, B7 (multi/main.f90:666-681)
-      const size_t g = (size_t)i + (size_t)n * j + nn * kz;
-      a.us[g] = uc + dt * (alpha * ru - beta * ruo);
-      a.vs[g] = vc + dt * (alpha * rv - beta * rvo);
-      a.ws[g] = wc + dt * (alpha * rw - beta * rwo);
-      a.ru[g] = ru;
-      a.rv[g] = rv;
-      a.rw[g] = rw;
     }
     // rotate: the slot of plane m-2 takes plane m+PD+1 at the next iteration
     const int t = sl[0];
@@ -469,9 +499,14 @@ __device__ __forceinline__ void momentum_body(const StencilArgs<T>& a, int KZ, i
 // ============================================================ projection
 // C2 + R1 (multi/main.f90:873-903): u = ustar - dt/rho*(p - p_m)*dxi, with the
 // sums and maxima of the projected u, v, w reduced per CTA in FP64.
-constexpr int PKZ = 16;
+// z planes per projection CTA: 64 where n allows, else 32 or 16 (512^3:
+// FP64 projection plus finalize 1.47 -> 1.41 ms against 16 planes, with a
+// quarter of the partials to reduce; FP32 projection 1.85 -> 1.49 ms).  The
+// FP64 loop takes it as a compile-time trip count (a run-time one measured
+// 1.79 ms there).
+__host__ __device__ constexpr int project_kz(int n) { return n % 64 == 0 ? 64 : (n % 32 == 0 ? 32 : 16); }
 
-template <class T>
+template <class T, int PKZ>
 __device__ __forceinline__ void project_body(const StencilArgs<T>& a, int bx, int by, int bz, int gx, int gy) {
   if (a.ctrl->status) return;
   const int n = a.c.n;
@@ -544,7 +579,7 @@ __device__ __forceinline__ void project_refine_body(const StencilArgs<float>& a,
   const int n = a.c.n;
   const double dtr = a.c.dtr, dxi = a.c.dxi;
   const int i = bx * TX + threadIdx.x % TX, j = by * TY + threadIdx.x / TX;
-  const int k0 = bz * PKZ;
+  const int pkz = project_kz(n), k0 = bz * pkz;
   const int im = i ? i - 1 : n - 1, jm = j ? j - 1 : n - 1;
   const int ip = (i + 1 == n) ? 0 : i + 1, jp = (j + 1 == n) ? 0 : j + 1;
   const size_t nn = (size_t)n * n;
@@ -556,7 +591,7 @@ __device__ __forceinline__ void project_refine_body(const StencilArgs<float>& a,
   double pm = P(col + nn * wrapi(k0 - 1, n));
   double pc = P(col + nn * k0);
   double wsc = (double)a.ws[col + nn * k0];
-  for (int k = k0; k < k0 + PKZ; ++k) {
+  for (int k = k0; k < k0 + pkz; ++k) {
     const size_t g = col + nn * k;
     const int kp = (k + 1 == n) ? 0 : k + 1;
     const size_t gzp = col + nn * kp;
@@ -678,12 +713,12 @@ __global__ void __launch_bounds__(PNT, 2) phase_kernel(StencilArgs<T> a, int KZ)
   phase_body<T>(a, KZ, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 template <class T, bool PF, int MTYv>
-__global__ void __launch_bounds__(TX * MTYv, momentum_min_blocks(PF, MTYv)) momentum_kernel(StencilArgs<T> a, int KZ) {
+__global__ void __launch_bounds__(TX * 8, momentum_min_blocks(PF, MTYv)) momentum_kernel(StencilArgs<T> a, int KZ) {
   momentum_body<T, PF, MTYv>(a, KZ, blockIdx.x, blockIdx.y, blockIdx.z);
 }
-template <class T>
+template <class T, int PKZ>
 __global__ void __launch_bounds__(NT, 4) project_kernel(StencilArgs<T> a) {
-  project_body<T>(a, blockIdx.x, blockIdx.y, blockIdx.z, gridDim.x, gridDim.y);
+  project_body<T, PKZ>(a, blockIdx.x, blockIdx.y, blockIdx.z, gridDim.x, gridDim.y);
 }
 __global__ void __launch_bounds__(NT) project_refine_kernel(StencilArgs<float> a, const float* __restrict__ dp) {
   project_refine_body(a, dp, blockIdx.x, blockIdx.y, blockIdx.z, gridDim.x, gridDim.y);
@@ -707,7 +742,7 @@ __global__ void __launch_bounds__(PNT, 2) phase_kernel_b(const SlotArgs<T>* __re
   phase_body<T>(a, KZ, blockIdx.x, blockIdx.y, blockIdx.z - sl * zch);
 }
 template <class T, bool PF, int MTYv>
-__global__ void __launch_bounds__(TX * MTYv, momentum_min_blocks(PF, MTYv)) momentum_kernel_b(const SlotArgs<T>* __restrict__ slots, int KZ,
+__global__ void __launch_bounds__(TX * 8, momentum_min_blocks(PF, MTYv)) momentum_kernel_b(const SlotArgs<T>* __restrict__ slots, int KZ,
                                                                          int zch) {
   const int sl = blockIdx.z / zch;
   if (!slots[sl].active) return;
@@ -715,11 +750,11 @@ __global__ void __launch_bounds__(TX * MTYv, momentum_min_blocks(PF, MTYv)) mome
   if (PF) a.phi_in = slots[sl].phi[(int)((a.ctrl->nstep + 1) & 1)];  // the updated phi
   momentum_body<T, PF, MTYv>(a, KZ, blockIdx.x, blockIdx.y, blockIdx.z - sl * zch);
 }
-template <class T>
+template <class T, int PKZ>
 __global__ void __launch_bounds__(NT, 4) project_kernel_b(const SlotArgs<T>* __restrict__ slots, int zch) {
   const int sl = blockIdx.z / zch;
   if (!slots[sl].active) return;
-  project_body<T>(slots[sl].st, blockIdx.x, blockIdx.y, blockIdx.z - sl * zch, gridDim.x, gridDim.y);
+  project_body<T, PKZ>(slots[sl].st, blockIdx.x, blockIdx.y, blockIdx.z - sl * zch, gridDim.x, gridDim.y);
 }
 __global__ void __launch_bounds__(NT) project_refine_kernel_b(const SlotArgs<float>* __restrict__ slots, int zch) {
   const int sl = blockIdx.z / zch;
@@ -763,10 +798,10 @@ template <class T> static size_t momentum_smem(bool pf, int mty) {
 }
 
 int stencil_size_ok(int n) {
-  return n >= 32 && n % TX == 0 && n % TY == 0 && n % PTY == 0 && n % PKZ == 0 && n % pick_kz(n) == 0;
+  return n >= 32 && n % TX == 0 && n % TY == 0 && n % PTY == 0 && n % project_kz(n) == 0 && n % pick_kz(n) == 0;
 }
 
-int project_partials(int n) { return (n / TX) * (n / TY) * (n / PKZ); }
+int project_partials(int n) { return (n / TX) * (n / TY) * (n / project_kz(n)); }
 
 template <class T> static cudaError_t prep_t() {
   cudaError_t e;
@@ -811,22 +846,26 @@ template <class T> cudaError_t launch_momentum(const StencilArgs<T>& a, bool pf,
     if (pf) momentum_kernel<T, true, 8><<<grid, TX * 8, sm, st>>>(a, kz);
     else momentum_kernel<T, false, 8><<<grid, TX * 8, sm, st>>>(a, kz);
   } else {
-    if (pf) momentum_kernel<T, true, 16><<<grid, TX * 16, sm, st>>>(a, kz);
-    else momentum_kernel<T, false, 16><<<grid, TX * 16, sm, st>>>(a, kz);
+    if (pf) momentum_kernel<T, true, 16><<<grid, TX * 8, sm, st>>>(a, kz);
+    else momentum_kernel<T, false, 16><<<grid, TX * 8, sm, st>>>(a, kz);
   }
   return cudaGetLastError();
 }
 
 template <class T> cudaError_t launch_project(const StencilArgs<T>& a, cudaStream_t st) {
   const int n = a.c.n;
-  dim3 grid(n / TX, n / TY, n / PKZ);
-  project_kernel<T><<<grid, NT, 0, st>>>(a);
+  dim3 grid(n / TX, n / TY, n / project_kz(n));
+  switch (project_kz(n)) {
+    case 64: project_kernel<T, 64><<<grid, NT, 0, st>>>(a); break;
+    case 32: project_kernel<T, 32><<<grid, NT, 0, st>>>(a); break;
+    default: project_kernel<T, 16><<<grid, NT, 0, st>>>(a); break;
+  }
   return cudaGetLastError();
 }
 
 cudaError_t launch_project_refine(const StencilArgs<float>& a, const float* dp, cudaStream_t st) {
   const int n = a.c.n;
-  dim3 grid(n / TX, n / TY, n / PKZ);
+  dim3 grid(n / TX, n / TY, n / project_kz(n));
   project_refine_kernel<<<grid, NT, 0, st>>>(a, dp);
   return cudaGetLastError();
 }
@@ -864,18 +903,22 @@ cudaError_t launch_momentum_batched(const SlotArgs<T>* slots, int nslots, int n,
     if (pf) momentum_kernel_b<T, true, 8><<<grid, TX * 8, sm, st>>>(slots, kz, n / kz);
     else momentum_kernel_b<T, false, 8><<<grid, TX * 8, sm, st>>>(slots, kz, n / kz);
   } else {
-    if (pf) momentum_kernel_b<T, true, 16><<<grid, TX * 16, sm, st>>>(slots, kz, n / kz);
-    else momentum_kernel_b<T, false, 16><<<grid, TX * 16, sm, st>>>(slots, kz, n / kz);
+    if (pf) momentum_kernel_b<T, true, 16><<<grid, TX * 8, sm, st>>>(slots, kz, n / kz);
+    else momentum_kernel_b<T, false, 16><<<grid, TX * 8, sm, st>>>(slots, kz, n / kz);
   }
   return cudaGetLastError();
 }
 template <class T>
 cudaError_t launch_project_batched(const SlotArgs<T>* slots, int nslots, int n, cudaStream_t st) {
-  dim3 grid(n / TX, n / TY, (n / PKZ) * nslots);
-  if constexpr (sizeof(T) == 8)
-    project_kernel_b<T><<<grid, NT, 0, st>>>(slots, n / PKZ);
-  else
-    project_refine_kernel_b<<<grid, NT, 0, st>>>(slots, n / PKZ);
+  dim3 grid(n / TX, n / TY, (n / project_kz(n)) * nslots);
+  if constexpr (sizeof(T) == 8) {
+    switch (project_kz(n)) {
+      case 64: project_kernel_b<T, 64><<<grid, NT, 0, st>>>(slots, n / project_kz(n)); break;
+      case 32: project_kernel_b<T, 32><<<grid, NT, 0, st>>>(slots, n / project_kz(n)); break;
+      default: project_kernel_b<T, 16><<<grid, NT, 0, st>>>(slots, n / project_kz(n)); break;
+    }
+  } else
+    project_refine_kernel_b<<<grid, NT, 0, st>>>(slots, n / project_kz(n));
   return cudaGetLastError();
 }
 template cudaError_t launch_project_batched<double>(const SlotArgs<double>*, int, int, cudaStream_t);
