@@ -53,8 +53,8 @@ ALGO_BYTES_STEP = {"fp64": {True: 280, False: 232}, "fp32": {True: 200, False: 1
 # stencil or column pass touches every point the same way at any size, so
 # traffic scales with the points processed; a full 512^3 capture is too large
 # to take under ncu.
-DRAM_BYTES_PER_POINT_FP64 = {"momentum": 104.07, "phase": 40.23, "project": 54.11, "xfwd": 30.84,
-                             "yfwd": 13.49, "zsolve": 13.50, "yinv": 13.49, "xinv": 13.93}
+DRAM_BYTES_PER_POINT_FP64 = {"momentum": 103.91, "phase": 40.55, "project": 54.13, "xfwd": 30.80,
+                             "yfwd": 13.59, "zsolve": 13.64, "yinv": 13.59, "xinv": 13.82}
 
 
 def kernel_bytes_per_point(n: int, pf: bool, precision: str = "fp64") -> dict:
