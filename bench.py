@@ -70,6 +70,7 @@ def kernel_bytes_per_point(n: int, pf: bool, precision: str = "fp64") -> dict:
         "yinv": 2 * spec,
         "xinv": spec + e,                         # read spectrum; write p (p0)
         "project": 7 * e,                         # read p, ustar(3); write u,v,w
+        "xinvproj": spec + 6 * e,                 # fused: read spectrum, ustar(3); write u,v,w
         "finalize": 0.0,
     }
     if precision != "fp64":

@@ -49,6 +49,10 @@ struct mhit_handle {
   double *fsin = nullptr, *fcos = nullptr;
   double* partials = nullptr;
   int nparts = 0;
+  // FP64 step with the fused x inverse + projection: p is not stored by the
+  // step; the spectrum still holds the last step's y-inverse output, from
+  // which mhit_get_pressure recomputes p.
+  bool p_in_spec = false;
   double* stat_partials = nullptr;
   double* stat_out = nullptr;
   double* h_stat = nullptr;  // pinned
@@ -189,9 +193,13 @@ std::vector<Stage> step_stages(mhit_handle* h, int cur) {
     pa.us = h->us; pa.vs = h->vs; pa.ws = h->ws;
     pa.spec = h->spec; pa.p = h->p; pa.tw = h->tw; pa.k2tab = h->k2tab; pa.ctrl = h->ctrl;
     pa.cdiv = h->c.cdiv; pa.ddxi = h->c.ddxi;
-    for (int k = 0; k < 5; ++k)
+    const bool fused = mhit::fused_projection(n) != 0;
+    for (int k = 0; k < (fused ? 4 : 5); ++k)
       v.push_back({pnames[k], [pa, n, k, st] { return mhit::launch_poisson_stage<double>(n, pa, k, st); }});
-    v.push_back({"project", [a, st] { return mhit::launch_project<double>(a, st); }});
+    if (fused)
+      v.push_back({"xinvproj", [pa, a, n, st] { return mhit::launch_xinv_project(n, pa, a, st); }});
+    else
+      v.push_back({"project", [a, st] { return mhit::launch_project<double>(a, st); }});
     Ctrl* ctrl = h->ctrl;
     double* part = h->partials;
     int np = h->nparts;
@@ -503,8 +511,11 @@ int mhit_create(const mhit_params* p, int nx, int ny, int nz, int precision, int
         break;
       }
     }
-    h->nparts = mhit::project_partials(n);
-    if ((e = dalloc(h, &h->partials, (size_t)h->nparts * 7 * sizeof(double)))) { fail(e, "cudaMalloc partials"); break; }
+    h->nparts = (precision == MHIT_FP64) ? mhit::step_partials_fp64(n) : mhit::project_partials(n);
+    if ((e = dalloc(h, &h->partials, (size_t)mhit::partials_capacity(n) * 7 * sizeof(double)))) {
+      fail(e, "cudaMalloc partials");
+      break;
+    }
     if ((e = dalloc(h, &h->ctrl, sizeof(Ctrl)))) { fail(e, "cudaMalloc ctrl"); break; }
     if ((e = dalloc(h, &h->stat_partials, (size_t)mhit::stats_partials(n) * 8 * sizeof(double))) ||
         (e = dalloc(h, &h->stat_out, 8 * sizeof(double))) || (e = cudaMallocHost(&h->h_stat, 8 * sizeof(double)))) {
@@ -600,6 +611,7 @@ int mhit_set_fields(mhit_handle* h, const double* u, const double* v, const doub
     CK(h, cudaMemsetAsync(h->fdp, 0, fb, h->st));
   } else {
     CK(h, cudaMemsetAsync(h->p, 0, fb, h->st));
+    h->p_in_spec = false;
   }
   reset_ctrl(h);
   CK(h, cudaMemcpyAsync(h->ctrl, h->h_ctrl, sizeof(Ctrl), cudaMemcpyHostToDevice, h->st));
@@ -652,6 +664,16 @@ int mhit_get_pressure(mhit_handle* h, double* p, int layout) {
       memcpy(t, a.data() + plane * k, plane * sizeof(double));
     }
   } else {
+    if (h->p_in_spec) {  // the last step's pressure: x inverse of its spectrum
+      mhit::PoissonArgs<double> pa;
+      pa.spec = h->spec;
+      pa.p = h->p;
+      pa.tw = h->tw;
+      pa.k2tab = h->k2tab;
+      pa.ctrl = nullptr;
+      CK(h, mhit::launch_poisson_stage<double>(h->n, pa, 4, h->st));
+      h->p_in_spec = false;
+    }
     CK(h, download(h, p, h->p, layout));
     CK(h, cudaStreamSynchronize(h->st));
   }
@@ -668,6 +690,7 @@ int mhit_step(mhit_handle* h, int nsteps, mhit_diag* out) {
     if (!h->graph[cur]) CK(h, build_graph(h, cur));
     CK(h, cudaGraphLaunch(h->graph[cur], h->st));
     ++h->nstep_host;
+    h->p_in_spec = !f32(h) && mhit::fused_projection(h->n);
   }
   CK(h, pull_ctrl(h));
   h->nstep_host = h->h_ctrl->nstep;  // fewer if a step raised the error status
@@ -685,6 +708,7 @@ int mhit_step_async(mhit_handle* h, int nsteps) {
     if (!h->graph[cur]) CK(h, build_graph(h, cur));
     CK(h, cudaGraphLaunch(h->graph[cur], h->st));
     ++h->nstep_host;
+    h->p_in_spec = !f32(h) && mhit::fused_projection(h->n);
   }
   return MHIT_OK;
 }
@@ -840,6 +864,7 @@ int mhit_profile_step(mhit_handle* h, int reps, double* ms, int* nstages) {
       CK(h, cudaEventRecord(ev[i + 1], h->st));
     }
     CK(h, cudaEventSynchronize(ev[NS]));
+    h->p_in_spec = !f32(h) && mhit::fused_projection(h->n);
     for (int i = 0; i < NS; ++i) {
       float t = 0;
       CK(h, cudaEventElapsedTime(&t, ev[i], ev[i + 1]));
@@ -875,6 +900,16 @@ int mhit_poisson_device(mhit_handle* h, const double* rhs_dev, double* p_dev) {
   pa.ctrl = nullptr;
   pa.cdiv = h->c.cdiv;
   pa.ddxi = h->c.ddxi;
+  if (h->p_in_spec) {
+    // keep the last step's pressure: recompute it before the spectrum is
+    // reused, unless the caller's buffers are the pressure buffer itself
+    if (rhs_dev != h->p && p_dev != h->p) {
+      mhit::PoissonArgs<double> px = pa;
+      px.p = h->p;
+      CK(h, mhit::launch_poisson_stage<double>(h->n, px, 4, h->st));
+    }
+    h->p_in_spec = false;
+  }
   CK(h, mhit::launch_poisson<double>(h->n, pa, h->st));
   return MHIT_OK;
 }

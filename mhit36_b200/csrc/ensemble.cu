@@ -317,7 +317,7 @@ size_t slot_bytes(int n, int pf, int precision) {
   const size_t N3 = (size_t)n * n * n, e = elem(precision);
   size_t fields = 9 + 1 + (pf ? 2 : 0) + (precision == MHIT_FP64 ? 0 : 1);  // + p / (p0, dp)
   const size_t spec = (size_t)n * n * mhit::spectrum_pitch(n, precision != MHIT_FP64) * 2 * e;
-  return fields * N3 * e + spec + (size_t)mhit::project_partials(n) * 7 * sizeof(double) + 2 * n * sizeof(double);
+  return fields * N3 * e + spec + (size_t)mhit::partials_capacity(n) * 7 * sizeof(double) + 2 * n * sizeof(double);
 }
 
 StepConst make_const(const mhit_params* p, int n) {
@@ -428,7 +428,7 @@ cudaError_t alloc_slot_buffers(mhit_ensemble* e, Class* c, SlotBuf& b) {
   const size_t spec = (size_t)n * n * mhit::spectrum_pitch(n, c->precision != MHIT_FP64) * 2 * el;
   if ((r = get(spec, &b.f[13]))) return r;
   if ((r = cudaMemsetAsync(b.f[13], 0, spec, c->st))) return r;
-  if ((r = get((size_t)mhit::project_partials(n) * 7 * sizeof(double), &b.f[14]))) return r;
+  if ((r = get((size_t)mhit::partials_capacity(n) * 7 * sizeof(double), &b.f[14]))) return r;
   void* t = nullptr;
   if ((r = get(2 * n * sizeof(double), &t))) return r;
   b.fsin = static_cast<double*>(t);
@@ -502,9 +502,14 @@ cudaError_t enqueue_class_step(Class* c, int kz, int mty) {
     const SlotArgs<double>* t = static_cast<const SlotArgs<double>*>(c->d_slots);
     if (c->pf && (err = mhit::launch_phase_batched<double>(t, S, n, kz, c->st))) return err;
     if ((err = mhit::launch_momentum_batched<double>(t, S, n, kz, c->pf != 0, c->st, mty))) return err;
-    for (int k = 0; k < 5; ++k)
+    const bool fused = mhit::fused_projection(n) != 0;  // x inverse fused into the projection
+    for (int k = 0; k < (fused ? 4 : 5); ++k)
       if ((err = mhit::launch_poisson_stage_batched<double>(t, S, n, k, 0, c->st))) return err;
-    if ((err = mhit::launch_project_batched<double>(t, S, n, c->st))) return err;
+    if (fused) {
+      if ((err = mhit::launch_xinv_project_batched(t, S, n, c->st))) return err;
+    } else if ((err = mhit::launch_project_batched<double>(t, S, n, c->st))) {
+      return err;
+    }
     return mhit::launch_finalize_batched(t, S, n, c->st);
   }
   const SlotArgs<float>* t = static_cast<const SlotArgs<float>*>(c->d_slots);

@@ -96,6 +96,18 @@ template <class T> cudaError_t launch_materialize(T* u, T* v, T* w, int n, Ctrl*
 cudaError_t prepare_stencils();
 int project_partials(int n);
 int stencil_size_ok(int n);
+// FP64 step with the x inverse fused into the projection (power-of-two
+// n >= 256): one kernel after the y inverse pass, writing its own partials.
+int fused_projection(int n);
+int xinv_project_partials(int n);
+cudaError_t launch_xinv_project(int n, const PoissonArgs<double>& pa, const StencilArgs<double>& a, cudaStream_t st);
+cudaError_t launch_xinv_project_batched(const SlotArgs<double>* slots, int nslots, int n, cudaStream_t st);
+// Partials the FP64 step's projection writes, and the buffer size that
+// holds either projection's partials (stride 7).
+inline int step_partials_fp64(int n) { return fused_projection(n) ? xinv_project_partials(n) : project_partials(n); }
+inline int partials_capacity(int n) {
+  return project_partials(n) > xinv_project_partials(n) ? project_partials(n) : xinv_project_partials(n);
+}
 
 template <class T>
 cudaError_t launch_stats(const T* u, const T* v, const T* w, const T* phi, const Ctrl* ctrl, int n, double dxi_c,

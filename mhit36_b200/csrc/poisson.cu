@@ -628,6 +628,208 @@ __device__ __forceinline__ void xfwd_reg_body(const T* __restrict__ us, const T*
   }
 }
 
+// ---------------------------------------------------------------- x inverse fused with the projection
+// FP64 step, power-of-two N >= 256 (C2 + R1 of multi/main.f90:812-903 in one
+// pass): p never goes to HBM.  A CTA owns the output rows j0 .. j0+2P-1 of
+// a chunk of KZ planes and marches through them.  Per plane it runs the x
+// inverse of its P line pairs plus one halo pair below (rows j0-2, j0-1;
+// the projection's backward difference in y needs row j0-1), puts the
+// plane's p rows into shared memory, and projects the plane:
+//   u = ustar - dt/rho*(p - p(i-1))*dxi, v with p(j-1), w with p(k-1),
+// where p(k-1) is the previous plane's rows, kept in a second buffer (the
+// chunk starts one plane early to fill it).  Per-CTA FP64 sums and maxima
+// as in project_body, in a fixed order.  The x inverse is xinv_reg_body's
+// arithmetic and the projection project_body's, so u, v, w and the
+// pressure (recomputed from the spectrum on request) are the same bits as
+// the unfused kernels give; only the grouping of the sums that make the
+// means differs.  Traffic per point: the half spectrum (8.06 B, plus the
+// halo rows, mostly L2 hits) + ustar, vstar, wstar + u, v, w: the 280 B/pt
+// schedule instead of 296.
+template <int N> struct XPCfg {
+  static constexpr bool ON = RCfg<N, double>::ON && N >= 256;
+  static constexpr int P = PCfg<N, double>::P;
+  static constexpr int TPC = N / 8;
+  static constexpr int NT = (P + 1) * TPC;  // a multiple of 32 for N >= 256
+  static constexpr int KZ = N >= 512 ? 16 : 8;
+  static constexpr size_t XBYTES = (size_t)(P + 1) * reg_rows(N) * sizeof(double2);  // exchange
+  static constexpr size_t PBYTES = (size_t)(2 * P + 1) * N * sizeof(double);         // plane's p rows
+  static constexpr size_t ABYTES = XBYTES > PBYTES ? XBYTES : PBYTES;                // the two alias
+  static constexpr size_t SMEM = ABYTES + (size_t)2 * P * N * sizeof(double);        // + previous plane
+  static constexpr int PARTS = (N / (2 * P)) * (N / KZ);
+};
+
+template <int N>
+__device__ __forceinline__ void xinvproj_body(const double2* __restrict__ spec, const double2* __restrict__ tw,
+                                              const StencilArgs<double>& a, int bx, int bz, int gx) {
+  typedef double2 C;
+  typedef XPCfg<N> X;
+  constexpr int P = X::P, TPC = X::TPC, NT = X::NT, KZ = X::KZ, RS = reg_rows(N);
+  constexpr size_t PITCH = PCfg<N, double>::PITCH;
+  static_assert(NT % 32 == 0, "whole warps");
+  if (a.ctrl->status) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* sx = reinterpret_cast<C*>(smem_raw);
+  double* sp = reinterpret_cast<double*>(smem_raw);  // the plane's p rows, after its transform
+  double* spp = reinterpret_cast<double*>(smem_raw + X::ABYTES);  // the previous plane's rows
+  const int t = threadIdx.x % TPC, q = threadIdx.x / TPC;        // q == P: the halo pair
+  const int j0 = bx * (2 * P), k0 = bz * KZ;
+  const int ja = (q < P) ? j0 + 2 * q : (j0 - 2 + N) % N;
+  const double dtr = a.c.dtr, dxi = a.c.dxi;
+  const size_t nn = (size_t)N * N;
+  const double* __restrict__ us = a.us;
+  const double* __restrict__ vs = a.vs;
+  const double* __restrict__ ws = a.ws;
+  double* __restrict__ uo_ = a.uo;
+  double* __restrict__ vo_ = a.vo;
+  double* __restrict__ wo_ = a.wo;
+  constexpr int PIT = (2 * P * N + NT - 1) / NT;  // projection points per thread and plane
+  constexpr int PG = 4;
+  double su = 0, sv = 0, sw = 0;
+  double xu = -INFINITY, xv = -INFINITY, xw = -INFINITY;
+  const int base = q * RS;
+  const auto at = [base](int n) { return base + reg_pad(n); };
+  for (int kk = k0 - 1; kk < k0 + KZ; ++kk) {
+    const int kw = (kk + N) % N;
+    // (1) x inverse of the plane's line pairs (xinv_reg_body)
+    const C* row = spec + ((size_t)kw * N + ja) * PITCH;
+    C A[8], B[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const int n = t + TPC * m;
+      const int h = (n <= N / 2) ? n : N - n;
+      A[m] = row[h];
+      B[m] = row[PITCH + h];
+    }
+    C v[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const int n = t + TPC * m;
+      C ca = A[m], cb = B[m];
+      if (n == 0 || n == N / 2) {
+        ca.y = 0;
+        cb.y = 0;
+      }
+      if (n <= N / 2) {
+        v[m].x = ca.x - cb.y;
+        v[m].y = ca.y + cb.x;
+      } else {
+        v[m].x = ca.x + cb.y;
+        v[m].y = cb.x - ca.y;
+      }
+    }
+    reg_fft_stages<N, 1, +1>(v, sx, tw, t, at);  // ends with a barrier: sx is free
+    // (2) the plane's p rows: row 0 = j0-1 (second line of the halo pair),
+    // rows 1 .. 2P = j0 .. j0+2P-1
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const int n = t + TPC * m;
+      if (q < P) {
+        sp[(2 * q + 1) * N + n] = v[m].x;
+        sp[(2 * q + 2) * N + n] = v[m].y;
+      } else {
+        sp[n] = v[m].y;
+      }
+    }
+    __syncthreads();
+    // (3) projection of plane kw (the chunk's first pass only fills spp).
+    // A thread's points are tid + NT*it; they are taken in groups of PG
+    // whose ustar/vstar/wstar loads are all issued before the group's
+    // arithmetic and stores (ustar and u are distinct arrays), so that a
+    // group costs one memory latency rather than PG.
+    if (kk >= k0) {
+#pragma unroll 1
+      for (int it0 = 0; it0 < PIT; it0 += PG) {
+        double lu[PG], lv[PG], lw[PG];
+#pragma unroll
+        for (int c = 0; c < PG; ++c) {
+          const int pi = threadIdx.x + NT * (it0 + c);
+          if (pi < 2 * P * N) {
+            const int x = pi % N, r = pi / N;
+            const size_t g = (size_t)x + (size_t)N * (j0 + r) + nn * kw;
+            lu[c] = us[g];
+            lv[c] = vs[g];
+            lw[c] = ws[g];
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < PG; ++c) {
+          const int pi = threadIdx.x + NT * (it0 + c);
+          if (pi < 2 * P * N) {
+            const int x = pi % N, r = pi / N;
+            const double pc = sp[(r + 1) * N + x];
+            const double pxm = sp[(r + 1) * N + (x ? x - 1 : N - 1)];
+            const double pym = sp[r * N + x];
+            const double pzm = spp[r * N + x];
+            const size_t g = (size_t)x + (size_t)N * (j0 + r) + nn * kw;
+            const double uo = lu[c] - dtr * (pc - pxm) * dxi;
+            const double vo = lv[c] - dtr * (pc - pym) * dxi;
+            const double wo = lw[c] - dtr * (pc - pzm) * dxi;
+            uo_[g] = uo;
+            vo_[g] = vo;
+            wo_[g] = wo;
+            su += uo;
+            sv += vo;
+            sw += wo;
+            xu = fmax(xu, uo);
+            xv = fmax(xv, vo);
+            xw = fmax(xw, wo);
+            // NaN must not vanish in fmax: fold it into the sums too
+            if (uo != uo || vo != vo || wo != wo) su = NAN;
+            spp[r * N + x] = pc;
+          }
+        }
+      }
+    } else {
+      for (int pi = threadIdx.x; pi < 2 * P * N; pi += NT) spp[pi] = sp[N + pi];
+    }
+    __syncthreads();  // sp (which aliases sx) is free for the next transform
+  }
+  // deterministic block reduction: xor-shuffle in warps, then warps in order
+  double vals[6] = {su, sv, sw, xu, xv, xw};
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) vals[c] += __shfl_xor_sync(0xffffffffu, vals[c], o);
+#pragma unroll
+    for (int c = 3; c < 6; ++c) vals[c] = fmax(vals[c], __shfl_xor_sync(0xffffffffu, vals[c], o));
+  }
+  __shared__ double red[NT / 32][6];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) red[wid][c] = vals[c];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double r6[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) r6[c] = red[0][c];
+    for (int w = 1; w < NT / 32; ++w) {
+      for (int c = 0; c < 3; ++c) r6[c] += red[w][c];
+      for (int c = 3; c < 6; ++c) r6[c] = fmax(r6[c], red[w][c]);
+    }
+    const size_t b = (size_t)bx + (size_t)gx * bz;
+    for (int c = 0; c < 6; ++c) a.partials[b * 6 + c] = r6[c];
+  }
+}
+
+template <int N>
+__global__ void __launch_bounds__(XPCfg<N>::NT, 2) xinvproj_kernel(const double2* __restrict__ spec,
+                                                                   const double2* __restrict__ tw,
+                                                                   StencilArgs<double> a) {
+  if constexpr (XPCfg<N>::ON) xinvproj_body<N>(spec, tw, a, blockIdx.x, blockIdx.y, gridDim.x);
+}
+template <int N>
+__global__ void __launch_bounds__(XPCfg<N>::NT, 2) xinvproj_kernel_b(const SlotArgs<double>* __restrict__ slots,
+                                                                     int zch) {
+  if constexpr (XPCfg<N>::ON) {
+    const int sl = blockIdx.y / zch;
+    if (!slots[sl].active) return;
+    xinvproj_body<N>(slots[sl].po.spec, slots[sl].po.tw, slots[sl].st, blockIdx.x, blockIdx.y - sl * zch,
+                     gridDim.x);
+  }
+}
+
 // ---------------------------------------------------------------- entry points
 // Single solve: block coordinates are the grid's.
 template <int N, int MODE, class T>
@@ -766,6 +968,11 @@ template <int N, class T> static cudaError_t set_attrs() {
     if ((e = cudaFuncSetAttribute(rcol_kernel_b<N, 1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, rs))) return e;
     if ((e = cudaFuncSetAttribute(rcol_kernel_b<N, 2, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, rs))) return e;
   }
+  if constexpr (sizeof(T) == 8 && XPCfg<N>::ON) {
+    const int xs2 = (int)XPCfg<N>::SMEM;
+    if ((e = cudaFuncSetAttribute(xinvproj_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, xs2))) return e;
+    if ((e = cudaFuncSetAttribute(xinvproj_kernel_b<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, xs2))) return e;
+  }
   return cudaSuccess;
 }
 
@@ -796,6 +1003,25 @@ static cudaError_t poisson_run(const PoissonArgs<T>& a, cudaStream_t st) {
   launch_col<N, 1, T>(a, st);
   xinv_kernel<N, T><<<gx, XCfg<N, T>::NT, xs, st>>>(a.spec, a.p, a.tw, a.ctrl);
   return cudaGetLastError();
+}
+
+template <int N>
+static cudaError_t xinvproj_run(const PoissonArgs<double>& pa, const StencilArgs<double>& a, cudaStream_t st) {
+  if constexpr (XPCfg<N>::ON) {
+    const dim3 grid(N / (2 * XPCfg<N>::P), N / XPCfg<N>::KZ);
+    xinvproj_kernel<N><<<grid, XPCfg<N>::NT, XPCfg<N>::SMEM, st>>>(pa.spec, pa.tw, a);
+    return cudaGetLastError();
+  }
+  return cudaErrorInvalidValue;
+}
+template <int N>
+static cudaError_t xinvproj_run_b(const SlotArgs<double>* slots, int nslots, cudaStream_t st) {
+  if constexpr (XPCfg<N>::ON) {
+    const dim3 grid(N / (2 * XPCfg<N>::P), (N / XPCfg<N>::KZ) * nslots);
+    xinvproj_kernel_b<N><<<grid, XPCfg<N>::NT, XPCfg<N>::SMEM, st>>>(slots, N / XPCfg<N>::KZ);
+    return cudaGetLastError();
+  }
+  return cudaErrorInvalidValue;
 }
 
 template <int N, class T>
@@ -893,6 +1119,54 @@ cudaError_t launch_poisson(int n, const PoissonArgs<T>& a, cudaStream_t st) {
 #undef MHIT_CASE
     default:
       return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_xinv_project(int n, const PoissonArgs<double>& pa, const StencilArgs<double>& a, cudaStream_t st) {
+  switch (n) {
+#define MHIT_CASE(NN) \
+  case NN:            \
+    return xinvproj_run<NN>(pa, a, st);
+    MHIT_FOR_SIZES(MHIT_CASE)
+#undef MHIT_CASE
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_xinv_project_batched(const SlotArgs<double>* slots, int nslots, int n, cudaStream_t st) {
+  switch (n) {
+#define MHIT_CASE(NN) \
+  case NN:            \
+    return xinvproj_run_b<NN>(slots, nslots, st);
+    MHIT_FOR_SIZES(MHIT_CASE)
+#undef MHIT_CASE
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+int fused_projection(int n) {
+  switch (n) {
+#define MHIT_CASE(NN) \
+  case NN:            \
+    return XPCfg<NN>::ON ? 1 : 0;
+    MHIT_FOR_SIZES(MHIT_CASE)
+#undef MHIT_CASE
+    default:
+      return 0;
+  }
+}
+
+int xinv_project_partials(int n) {
+  switch (n) {
+#define MHIT_CASE(NN) \
+  case NN:            \
+    return XPCfg<NN>::ON ? XPCfg<NN>::PARTS : 0;
+    MHIT_FOR_SIZES(MHIT_CASE)
+#undef MHIT_CASE
+    default:
+      return 0;
   }
 }
 

@@ -924,7 +924,7 @@ cudaError_t launch_project_batched(const SlotArgs<T>* slots, int nslots, int n, 
 template cudaError_t launch_project_batched<double>(const SlotArgs<double>*, int, int, cudaStream_t);
 template cudaError_t launch_project_batched<float>(const SlotArgs<float>*, int, int, cudaStream_t);
 cudaError_t launch_finalize_batched(const SlotArgs<double>* slots, int nslots, int n, cudaStream_t st) {
-  finalize_kernel_b<double><<<nslots, FNT, 0, st>>>(slots, project_partials(n), 6);
+  finalize_kernel_b<double><<<nslots, FNT, 0, st>>>(slots, step_partials_fp64(n), 6);
   return cudaGetLastError();
 }
 cudaError_t launch_finalize_batched_f32(const SlotArgs<float>* slots, int nslots, int n, cudaStream_t st) {

@@ -77,6 +77,21 @@ def test_continuous_admission_with_few_slots():
         assert admits[2] >= min(admits[:2])
 
 
+def test_fused_projection_class_matches_solver_bitwise():
+    """From 256^3 the FP64 step fuses the x inverse into the projection, in
+    the batched class graph as in the plain Solver; two requests of one
+    class (one with ACDI) must still match their solo runs bit for bit."""
+    from mhit36_b200.ensemble import Ensemble
+    cases = [_case(256, True, 21), _case(256, False, 22)]
+    with Ensemble(slots_per_class=2) as ens:
+        a = ens.submit(256, _params(dt=2e-4), *cases[0], nsteps=3)
+        b = ens.submit(256, _params(dt=2e-4, mu=3e-3), *cases[1], nsteps=2)
+        ens.run()
+        assert ens.query(a)["state"] == "done" and ens.query(b)["state"] == "done"
+        _same(ens.result(a), _solo(256, _params(dt=2e-4), cases[0], 3))
+        _same(ens.result(b), _solo(256, _params(dt=2e-4, mu=3e-3), cases[1], 2))
+
+
 def test_fp32_form_in_ensemble_matches_solver():
     from mhit36_b200.ensemble import Ensemble
     p = _params(k2_mode=1)

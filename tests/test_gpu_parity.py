@@ -236,10 +236,14 @@ def test_phi_volume_conserved_and_bounded():
 
 
 def test_ns_acdi_256_3_steps():
-    """256^3 NS+ACDI (8 drops) against the oracle: exercises the 8x8x4 radix plan."""
+    """256^3 NS+ACDI (8 drops) against the oracle: exercises the 8x8x4 radix
+    plan and the x inverse fused into the projection, whose pressure is
+    recomputed from the last step's spectrum on request."""
     p = _params()
-    ref, got, od, d, _, _ = run_pair(256, 3, True, p)
+    ref, got, od, d, pref, pgot = run_pair(256, 3, True, p)
     _check(ref, got, True)
+    assert rel_err(pgot, pref) <= 1e-11
+    assert abs(d["umax"] - od["umax"]) <= 1e-12 * abs(od["umax"])
 
 
 @pytest.mark.parametrize("n", [256, 512])
