@@ -54,7 +54,7 @@ ALGO_BYTES_STEP = {"fp64": {True: 280, False: 232}, "fp32": {True: 200, False: 1
 # traffic scales with the points processed; a full 512^3 capture is too large
 # to take under ncu.
 DRAM_BYTES_PER_POINT_FP64 = {"momentum": 103.91, "phase": 40.55, "project": 54.13, "xfwd": 30.80,
-                             "yfwd": 13.59, "zsolve": 13.64, "yinv": 13.59, "xinv": 13.82}
+                             "yfwd": 13.59, "zsolve": 13.64, "yinv": 13.59, "xinv": 13.82, "xinvproj": 55.30}
 
 
 def kernel_bytes_per_point(n: int, pf: bool, precision: str = "fp64") -> dict:
