@@ -290,11 +290,7 @@ __global__ void __launch_bounds__(256, 2) colpass_kernel_b(const SlotArgs<T>* __
 template <int N, class T> struct RCfg {
   static constexpr int CC = PCfg<N, T>::CC;
   static constexpr int NT = CC * (N / 8);
-#ifdef MHIT_STAGED_COLUMNS
-  static constexpr bool ON = false;
-#else
   static constexpr bool ON = (N & (N - 1)) == 0;
-#endif
   // Resident CTAs per SM the kernels are built for: registers capped at 80
   // per thread in FP64 (3 CTAs of 256 threads), 64 in the FP32 y passes and
   // 40 in the FP32 z solve (measured on B200 at 512^3: the FP32 z solve
@@ -305,16 +301,17 @@ template <int N, class T> struct RCfg {
   // 0.56 vs 0.66 ms), their extra buffer costing resident CTAs.  The twiddle
   // table sits in shared memory (reading it through L1 measured slower).
   static constexpr bool PF = sizeof(T) == 8;
-  static constexpr bool STW = true;
+  static constexpr bool stw(int kind) { return kind >= 0; }
   static constexpr int minb(int kind) {
     const int r = sizeof(T) == 8 ? (kind == 2 ? 128 : 80) : (kind == 2 ? 40 : 64);
     return 65536 / (NT * r) > 1 ? 65536 / (NT * r) : 1;
   }
 };
 
-template <int N, class T> static size_t rcolsmem() {  // exchange buffer, twiddle table, prefetch buffer
+template <int N, int KIND, class T> static size_t rcolsmem() {  // exchange buffer, twiddle table, prefetch buffer
   typedef RCfg<N, T> R;
-  return ((size_t)reg_rows(N) * R::CC + (R::STW ? N : 0) + (R::PF ? 8 * R::NT : 0)) * sizeof(typename C2<T>::t);
+  return ((size_t)reg_rows(N) * R::CC + (R::stw(KIND) ? N : 0) + (R::PF ? 8 * R::NT : 0)) *
+         sizeof(typename C2<T>::t);
 }
 
 template <int N, int KIND, class T, class Getter>
@@ -325,10 +322,10 @@ __device__ __forceinline__ void rcol_run(int total, const typename C2<T>::t* __r
   constexpr int NT = RCfg<N, T>::NT;
   C* s = reinterpret_cast<C*>(smem_raw);
   C* stw = s + reg_rows(N) * CC;
-  C* pbuf = stw + (RCfg<N, T>::STW ? N : 0);
+  C* pbuf = stw + (RCfg<N, T>::stw(KIND) ? N : 0);
   if ((int)blockIdx.x >= total) return;
   const C* tw = gtw;
-  if constexpr (RCfg<N, T>::STW) {
+  if constexpr (RCfg<N, T>::stw(KIND)) {
     for (int q = threadIdx.x; q < N; q += NT) stw[q] = gtw[q];
     __syncthreads();
     tw = stw;
@@ -913,9 +910,10 @@ template <int N, int KIND, class T, bool BATCHED> static int rcolgrid() {
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (BATCHED)
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, rcol_kernel_b<N, KIND, T>, RCfg<N, T>::NT,
-                                                    rcolsmem<N, T>());
+                                                    rcolsmem<N, KIND, T>());
     else
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, rcol_kernel<N, KIND, T>, RCfg<N, T>::NT, rcolsmem<N, T>());
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, rcol_kernel<N, KIND, T>, RCfg<N, T>::NT,
+                                                    rcolsmem<N, KIND, T>());
     grid = std::max(1, sms) * std::max(1, per);
   }
   return grid;
@@ -925,7 +923,7 @@ template <int N, int KIND, class T, bool BATCHED> static int rcolgrid() {
 // register-resident transform for power-of-two N, the staged one otherwise.
 template <int N, int KIND, class T> static void launch_col(const PoissonArgs<T>& a, cudaStream_t st) {
   if constexpr (RCfg<N, T>::ON)
-    rcol_kernel<N, KIND, T><<<rcolgrid<N, KIND, T, false>(), RCfg<N, T>::NT, rcolsmem<N, T>(), st>>>(
+    rcol_kernel<N, KIND, T><<<rcolgrid<N, KIND, T, false>(), RCfg<N, T>::NT, rcolsmem<N, KIND, T>(), st>>>(
         a.spec, a.tw, a.k2tab, a.ctrl);
   else
     colpass_kernel<N, KIND, T><<<colgrid<N, KIND, T, false>(), PCfg<N, T>::NT, colsmem<N, T>(), st>>>(
@@ -934,7 +932,7 @@ template <int N, int KIND, class T> static void launch_col(const PoissonArgs<T>&
 template <int N, int KIND, class T>
 static void launch_col_b(const SlotArgs<T>* slots, int nslots, int which, cudaStream_t st) {
   if constexpr (RCfg<N, T>::ON)
-    rcol_kernel_b<N, KIND, T><<<rcolgrid<N, KIND, T, true>(), RCfg<N, T>::NT, rcolsmem<N, T>(), st>>>(
+    rcol_kernel_b<N, KIND, T><<<rcolgrid<N, KIND, T, true>(), RCfg<N, T>::NT, rcolsmem<N, KIND, T>(), st>>>(
         slots, nslots, which);
   else
     colpass_kernel_b<N, KIND, T><<<colgrid<N, KIND, T, true>(), PCfg<N, T>::NT, colsmem<N, T>(), st>>>(
@@ -960,13 +958,14 @@ template <int N, class T> static cudaError_t set_attrs() {
     if ((e = cudaFuncSetAttribute(colpass_kernel_b<N, 1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps))) return e;
     if ((e = cudaFuncSetAttribute(colpass_kernel_b<N, 2, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps))) return e;
   } else {
-    const int rs = (int)rcolsmem<N, T>();
-    if ((e = cudaFuncSetAttribute(rcol_kernel<N, 0, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, rs))) return e;
-    if ((e = cudaFuncSetAttribute(rcol_kernel<N, 1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, rs))) return e;
-    if ((e = cudaFuncSetAttribute(rcol_kernel<N, 2, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, rs))) return e;
-    if ((e = cudaFuncSetAttribute(rcol_kernel_b<N, 0, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, rs))) return e;
-    if ((e = cudaFuncSetAttribute(rcol_kernel_b<N, 1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, rs))) return e;
-    if ((e = cudaFuncSetAttribute(rcol_kernel_b<N, 2, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, rs))) return e;
+    const int r0 = (int)rcolsmem<N, 0, T>(), r1 = (int)rcolsmem<N, 1, T>(), r2 = (int)rcolsmem<N, 2, T>();
+    const cudaFuncAttribute A = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    if ((e = cudaFuncSetAttribute(rcol_kernel<N, 0, T>, A, r0))) return e;
+    if ((e = cudaFuncSetAttribute(rcol_kernel<N, 1, T>, A, r1))) return e;
+    if ((e = cudaFuncSetAttribute(rcol_kernel<N, 2, T>, A, r2))) return e;
+    if ((e = cudaFuncSetAttribute(rcol_kernel_b<N, 0, T>, A, r0))) return e;
+    if ((e = cudaFuncSetAttribute(rcol_kernel_b<N, 1, T>, A, r1))) return e;
+    if ((e = cudaFuncSetAttribute(rcol_kernel_b<N, 2, T>, A, r2))) return e;
   }
   if constexpr (sizeof(T) == 8 && XPCfg<N>::ON) {
     const int xs2 = (int)XPCfg<N>::SMEM;
