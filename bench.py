@@ -121,40 +121,63 @@ def workload(n, pf, dt, precision="fp64"):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled during the timed region.
+
+    nvidia-smi takes a moment to start, so start() returns only once the
+    sampler has written its first row; the rows written after that (during
+    the timed region, plus the first one after it if the region was shorter
+    than the sampling period) are the ones reported."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    PERIOD_MS = 100
 
     def __init__(self, gpu_index: int):
         self.idx = gpu_index
         self.proc = None
         self.path = None
+        self.n0 = 0
+
+    def _rows(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) >= 9:
+                    rows.append(f)
+        except OSError:
+            pass
+        return rows
 
     def start(self):
         try:
             fd, self.path = tempfile.mkstemp(suffix=".csv")
             os.close(fd)
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", str(self.PERIOD_MS)],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        t0 = time.time()
+        while not self._rows() and time.time() - t0 < 10.0 and self.proc.poll() is None:
+            time.sleep(0.02)
+        self.n0 = len(self._rows())
 
     def stop(self):
         if self.proc is None:
             return None
+        t0 = time.time()
+        while len(self._rows()) <= self.n0 and time.time() - t0 < 3 * self.PERIOD_MS / 1000 and \
+                self.proc.poll() is None:
+            time.sleep(0.01)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
-        rows = []
-        for line in open(self.path):
-            f = [x.strip() for x in line.split(",")]
-            if len(f) >= 9:
-                rows.append(f)
+        rows = self._rows()[self.n0:]
         os.unlink(self.path)
         if not rows:
             return None

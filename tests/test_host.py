@@ -185,3 +185,26 @@ def test_vtk_export_format(tmp_path):
     assert np.array_equal(back["u"], u.astype(np.float32))
     assert np.array_equal(back["phi"], phi.astype(np.float32))
     assert abs(float(back["coords"][0][-1]) - 2 * np.pi) < 1e-6  # x(n) = 2 pi on the reference grid
+
+
+def test_clock_sampler_reports_rows_of_the_timed_region(tmp_path, monkeypatch):
+    """bench.py's clock record, against a stand-in nvidia-smi that prints one
+    CSV row per period (the real one only exists on the GPU box)."""
+    import sys
+    import time
+    sys.path.insert(0, ROOT)
+    import bench
+    fake = tmp_path / "nvidia-smi"
+    fake.write_text("#!/bin/sh\nsleep 0.3\nwhile true; do\n"
+                    "  echo '0, 1965, 1965, 700.5, 0x0000000000000004, Not Active, Not Active, Not Active, Active'\n"
+                    "  sleep 0.05\ndone\n")
+    fake.chmod(0o755)
+    monkeypatch.setenv("PATH", f"{tmp_path}:{os.environ['PATH']}")
+    s = bench.ClockSampler(0)
+    t0 = time.time()
+    s.start()
+    assert time.time() - t0 >= 0.25  # waited for the sampler's first row
+    time.sleep(0.2)
+    rec = s.stop()
+    assert rec["samples"] >= 1 and rec["sm_mhz"] == 1965.0 and rec["sm_max_mhz"] == 1965.0
+    assert rec["reasons"] == ["sw_power_cap"]
