@@ -132,7 +132,10 @@ int mhit_set_fields(mhit_handle* h, const double* u, const double* v, const doub
  * Halo cells of MHIT_LAYOUT_PIX_HALO are filled periodically. */
 int mhit_get_fields(mhit_handle* h, double* u, double* v, double* w, double* phi, int layout);
 
-/* Download the last pressure p (multi/main.f90:842-850). */
+/* Download the last pressure p (multi/main.f90:842-850).  From 256^3 up the
+ * FP64 step fuses the x inverse FFT into the projection and does not store
+ * p; this call then recomputes it from the last step's spectrum (one x
+ * inverse pass on the device) before the download. */
 int mhit_get_pressure(mhit_handle* h, double* p, int layout);
 
 /*
