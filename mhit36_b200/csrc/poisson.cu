@@ -291,17 +291,18 @@ template <int N, class T> struct RCfg {
   static constexpr int CC = PCfg<N, T>::CC;
   static constexpr int NT = CC * (N / 8);
   static constexpr bool ON = (N & (N - 1)) == 0;
-  // Resident CTAs per SM the kernels are built for: registers capped at 80
-  // per thread in FP64 (3 CTAs of 256 threads), 64 in the FP32 y passes and
-  // 40 in the FP32 z solve (measured on B200 at 512^3: the FP32 z solve
-  // 0.68 -> 0.57 ms at 40; uncapped or lower caps were slower elsewhere).
+  // Register caps per thread (via the resident CTAs per SM the kernels are
+  // built for): FP64 y passes 80 (3 CTAs of 256 threads), FP64 z solve 128
+  // (a cap of 80 spilled and measured 24% slower), FP32 y passes 64, FP32 z
+  // solve 40 (measured on B200 at 512^3: 0.68 -> 0.57 ms against no cap).
   // FP64: the next slab is prefetched into shared memory with cp.async while
   // the current one is transformed (512^3: y passes 0.48 -> 0.41 ms, z solve
   // 0.94 -> 0.88 ms); the FP32 passes are faster without (0.24 vs 0.25 and
   // 0.56 vs 0.66 ms), their extra buffer costing resident CTAs.  The twiddle
-  // table sits in shared memory (reading it through L1 measured slower).
+  // table sits in shared memory for every pass (reading it through L1
+  // measured slower for the y passes and no faster for the z solve).
   static constexpr bool PF = sizeof(T) == 8;
-  static constexpr bool stw(int kind) { return kind >= 0; }
+  static constexpr bool stw(int) { return true; }
   static constexpr int minb(int kind) {
     const int r = sizeof(T) == 8 ? (kind == 2 ? 128 : 80) : (kind == 2 ? 40 : 64);
     return 65536 / (NT * r) > 1 ? 65536 / (NT * r) : 1;
