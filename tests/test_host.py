@@ -208,3 +208,45 @@ def test_clock_sampler_reports_rows_of_the_timed_region(tmp_path, monkeypatch):
     rec = s.stop()
     assert rec["samples"] >= 1 and rec["sm_mhz"] == 1965.0 and rec["sm_max_mhz"] == 1965.0
     assert rec["reasons"] == ["sw_power_cap"]
+
+
+def test_integration_c_examples_compile_and_link(tmp_path):
+    """The C snippets of INTEGRATION.md compile against include/mhit.h and
+    every function they call resolves in libmhit.so (linked, not run)."""
+    import subprocess
+    from mhit36_b200 import capi
+    if not os.path.exists(capi.LIB_PATH):
+        pytest.skip("libmhit.so not built")
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    blocks = re.findall(r"```c\n(.*?)```", text, re.S)
+    assert len(blocks) >= 2
+    body = "\n".join(b.replace('#include "mhit.h"', "") for b in blocks)
+    src = ('#include "mhit.h"\n#include <stdint.h>\n'
+           "int example(double* u, double* v, double* w, double* phi) {\n" + body + "\nreturn rc;\n}\n"
+           "int main(void) { return 0; }\n")
+    c = tmp_path / "example.c"
+    c.write_text(src)
+    lib_dir = os.path.dirname(capi.LIB_PATH)
+    r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-Wno-unused-variable", "-I",
+                        os.path.join(ROOT, "include"), str(c), "-o", str(tmp_path / "example"), "-L", lib_dir,
+                        "-lmhit", "-Wl,--unresolved-symbols=ignore-in-shared-libs"],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+
+
+def test_integration_python_examples_parse_and_name_real_api():
+    """The Python snippets of INTEGRATION.md parse, and the package names
+    they import exist."""
+    import ast
+    import importlib
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    blocks = re.findall(r"```python\n(.*?)```", text, re.S)
+    assert blocks
+    for src in blocks:
+        tree = ast.parse(src)
+        for node in ast.walk(tree):
+            if isinstance(node, ast.ImportFrom) and node.module and node.module.startswith("mhit36_b200"):
+                mod = importlib.import_module(node.module)
+                for alias in node.names:
+                    assert hasattr(mod, alias.name) or importlib.util.find_spec(
+                        f"{node.module}.{alias.name}") is not None, (node.module, alias.name)
