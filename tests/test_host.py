@@ -250,3 +250,21 @@ def test_integration_python_examples_parse_and_name_real_api():
                 for alias in node.names:
                     assert hasattr(mod, alias.name) or importlib.util.find_spec(
                         f"{node.module}.{alias.name}") is not None, (node.module, alias.name)
+
+
+def test_serve_stream_follows_its_recipe():
+    """The served-ensemble stream: N over {64,96,128,192,256}, nu in
+    [3e-3, 1e-2], ACDI on for exactly half, 2-16 drops, 50-500 steps,
+    seeded (the same seed gives the same stream)."""
+    from mhit36_b200 import serve_bench
+    sizes = [64, 96, 128, 192, 256]
+    reqs, gaps = serve_bench.make_stream(256, 2024, sizes)
+    again, gaps2 = serve_bench.make_stream(256, 2024, sizes)
+    assert reqs == again and np.array_equal(gaps, gaps2)
+    assert {r["n"] for r in reqs} == set(sizes)
+    assert sum(r["pf"] for r in reqs) == 128
+    assert all(3e-3 <= r["nu"] <= 1e-2 and 2 <= r["ndrops"] <= 16 and 50 <= r["steps"] <= 500 for r in reqs)
+    assert len(gaps) == 256 and np.all(gaps > 0)
+    # the same replay of FIFO queueing the benchmark uses for the one-at-a-time arm
+    done, lat = serve_bench.replay_fifo(np.array([0.0, 0.5, 0.6]), np.array([1.0, 1.0, 1.0]))
+    assert np.allclose(done, [1.0, 2.0, 3.0]) and np.allclose(lat, [1.0, 1.5, 2.4])
