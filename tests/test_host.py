@@ -164,8 +164,11 @@ def test_create_without_gpu_fails_cleanly():
     if torch.cuda.is_available():
         pytest.skip("GPU present")
     from mhit36_b200 import Solver, MhitError
+    from mhit36_b200.ensemble import Ensemble
     with pytest.raises(MhitError):
         Solver(32, phase_field=False)
+    with pytest.raises(MhitError):  # no silent CPU fallback for the served ensemble either
+        Ensemble()
 
 
 def test_vtk_export_format(tmp_path):
