@@ -358,14 +358,20 @@ def main():
         ptr = [b.data_ptr() for b in hb] + ([None] if not pf else [])
         barrier()
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
+        # CUDA events on the solver's stream bracket the whole job: the uploads
+        # and downloads run on that stream, and every host pause between its
+        # operations shows as stream idle time inside the span
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
         s.set_fields_ptr(*ptr)
         for _ in range(args.steps):
             s.step(1)  # returns the step's diagnostics to the host
         s.get_fields_ptr(*ptr)
+        f1.record(stream)
+        f1.synchronize()
         torch.cuda.synchronize()
-        el = time.perf_counter() - t0
-        el = max_over_ranks(el, world)
+        el = max_over_ranks(f0.elapsed_time(f1) / 1e3, world)
         nf = len(hb)
         e2e = {"value": replicas_rate(world, npts, args.steps, el), "unit": UNIT,
                "h2d_bytes_per_step": nf * npts * 8 / args.steps,
