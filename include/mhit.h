@@ -248,9 +248,12 @@ const char* mhit_last_error(mhit_handle* h);
  * cudaMalloc/cudaFree: its scratch (half spectrum and tables) is a fixed
  * device array of the library for n <= MHIT_NOALLOC_MAX_N (18.9 MB, held on
  * every GPU that loads the library until exit).  Larger n returns
- * MHIT_ERR_SCRATCH_LIMIT.  The first call on a device resolves the scratch
- * address, so make it before any stream capture.  All calls share the
- * scratch: calls that overlap on the GPU race and must be serialised.
+ * MHIT_ERR_SCRATCH_LIMIT.  The first call on a device (with that device
+ * current) resolves the scratch address and fills the twiddle and k^2 tables
+ * of every supported size with one synchronous host-to-device copy, so make
+ * it before any stream capture; later calls only enqueue the solve's kernels
+ * on `stream`.  All calls share the scratch: calls that overlap on the GPU
+ * race and must be serialised.
  */
 #define MHIT_NOALLOC_MAX_N 128
 int mhit_poisson_noalloc(const double* rhs_dev, double* p_dev, int n, int k2_mode, int grid_mode,

@@ -14,16 +14,23 @@
 //
 // Set-up: the first call on a device, with that device current, looks up the
 // arrays' device addresses with cudaGetSymbolAddress (their names in host code
-// are only host-side stand-ins) and caches them; that first call should come
-// before any stream capture.  Every call shares the same arrays and leaves its
-// contents behind, so calls that overlap on the GPU (different streams, or
-// different host threads) race; serialise them.  Nothing in the scratch has to
-// start at zero: every element a solve reads is written earlier in the same
-// call (columns beyond kx = n/2 are transformed independently and zeroed by the
+// are only host-side stand-ins), fills the twiddle tables of every built size
+// up to the maximum and the k^2 tables of every (size, k2_mode, grid_mode)
+// with one synchronous copy, and opts those sizes' kernels into their shared
+// memory.  That first call should come before any stream capture.  After it,
+// a call only launches the solve's kernels on the caller's stream: nothing is
+// copied from the host.
+//
+// Every call shares the same spectrum array and leaves its contents behind,
+// so calls that overlap on the GPU (different streams, or different host
+// threads) race; serialise them.  Nothing in the spectrum has to start at
+// zero: every element a solve reads is written earlier in the same call
+// (columns beyond kx = n/2 are transformed independently and zeroed by the
 // k^2 division before anything reads them).
 #include <cuda_runtime.h>
 #include <math.h>
 #include <mutex>
+#include <vector>
 
 #include "internal.h"
 #include "mhit.h"
@@ -34,9 +41,35 @@ constexpr int kMaxN = MHIT_NOALLOC_MAX_N;
 constexpr size_t kPitchMax = (kMaxN / 2 + 1 + 7) / 8 * 8;  // spectrum row pitch for n = kMaxN
 constexpr size_t kSpecElems = (size_t)kMaxN * kMaxN * kPitchMax;
 
+// Built sizes up to kMaxN, and the offset of each size's tables.
+constexpr int kSizeSlots = 16;
+struct SizeTable {
+  int count = 0;
+  int n[kSizeSlots] = {};
+  int off[kSizeSlots] = {};
+  int total = 0;
+};
+constexpr SizeTable make_sizes() {
+  SizeTable t;
+#define MHIT_CASE(NN)            \
+  if (NN <= kMaxN) {             \
+    t.n[t.count] = NN;           \
+    t.off[t.count] = t.total;    \
+    t.total += NN;               \
+    ++t.count;                   \
+  }
+  MHIT_FOR_SIZES(MHIT_CASE)
+#undef MHIT_CASE
+  return t;
+}
+constexpr SizeTable kSizes = make_sizes();
+static_assert(kSizes.count > 0 && kSizes.count <= kSizeSlots, "size table");
+// k^2 tables: one per (k2_mode, grid_mode) for every size
+constexpr int kModes = 4;
+
 static __device__ __align__(256) double2 g_noalloc_spec[kSpecElems];
-static __device__ __align__(256) double2 g_noalloc_tw[kMaxN];
-static __device__ __align__(256) double g_noalloc_k2[kMaxN];
+static __device__ __align__(256) double2 g_noalloc_tw[kSizes.total];
+static __device__ __align__(256) double g_noalloc_k2[kModes * kSizes.total];
 
 constexpr int kMaxDevices = 64;
 struct Addrs {
@@ -48,25 +81,71 @@ struct Addrs {
 Addrs g_addrs[kMaxDevices];
 std::mutex g_mutex;
 
+int size_slot(int n) {
+  for (int q = 0; q < kSizes.count; ++q)
+    if (kSizes.n[q] == n) return q;
+  return -1;
+}
+
+int mode_index(int k2_mode, int grid_mode) {
+  return (k2_mode == MHIT_K2_FD ? 2 : 0) + (grid_mode == MHIT_GRID_CONSISTENT ? 1 : 0);
+}
+
+// The tables mhit_create builds for a handle, for every size and mode (the
+// same values, so a solve here equals mhit_poisson_device's bit for bit).
+void host_tables(std::vector<double2>& tw, std::vector<double>& k2) {
+  tw.assign(kSizes.total, double2{0, 0});
+  k2.assign((size_t)kModes * kSizes.total, 0.0);
+  const double twopi = 8.0 * atan(1.0);
+  const double lx = twopi;
+  const double pi = 4.0 * atan(1.0);
+  for (int q = 0; q < kSizes.count; ++q) {
+    const int n = kSizes.n[q], off = kSizes.off[q];
+    for (int m = 0; m < n; ++m) {
+      long double ang = 2.0L * 3.141592653589793238462643383279502884L * (long double)m / (long double)n;
+      tw[off + m].x = (double)cosl(ang);
+      tw[off + m].y = -(double)sinl(ang);
+    }
+    for (int k2_mode = 0; k2_mode < 2; ++k2_mode)
+      for (int grid_mode = 0; grid_mode < 2; ++grid_mode) {
+        double* t = k2.data() + (size_t)mode_index(k2_mode, grid_mode) * kSizes.total + off;
+        const double dx = (grid_mode == MHIT_GRID_CONSISTENT) ? lx / n : lx / (n - 1);
+        const double ddxi = 1.0 / dx / dx;
+        for (int m = 0; m < n; ++m) {
+          if (k2_mode == MHIT_K2_FD) {
+            const double s = sin(pi * m / n);
+            t[m] = (4.0 * ddxi) * (s * s);
+          } else {
+            const double kk = (m < n / 2 ? (double)m : (double)(m - n)) * (twopi / lx);
+            t[m] = kk * kk;
+          }
+        }
+      }
+  }
+}
+
 int setup_device(int dev, Addrs* out) {
   std::lock_guard<std::mutex> lock(g_mutex);
   Addrs& a = g_addrs[dev];
   if (!a.ready) {
-    if (cudaGetSymbolAddress((void**)&a.spec, g_noalloc_spec) != cudaSuccess) return MHIT_ERR_CUDA;
-    if (cudaGetSymbolAddress((void**)&a.tw, g_noalloc_tw) != cudaSuccess) return MHIT_ERR_CUDA;
-    if (cudaGetSymbolAddress((void**)&a.k2, g_noalloc_k2) != cudaSuccess) return MHIT_ERR_CUDA;
-    a.ready = true;
+    Addrs t;
+    if (cudaGetSymbolAddress((void**)&t.spec, g_noalloc_spec) != cudaSuccess) return MHIT_ERR_CUDA;
+    if (cudaGetSymbolAddress((void**)&t.tw, g_noalloc_tw) != cudaSuccess) return MHIT_ERR_CUDA;
+    if (cudaGetSymbolAddress((void**)&t.k2, g_noalloc_k2) != cudaSuccess) return MHIT_ERR_CUDA;
+    std::vector<double2> tw;
+    std::vector<double> k2;
+    host_tables(tw, k2);
+    if (cudaMemcpy(t.tw, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice) != cudaSuccess)
+      return MHIT_ERR_CUDA;
+    if (cudaMemcpy(t.k2, k2.data(), k2.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+      return MHIT_ERR_CUDA;
+    for (int q = 0; q < kSizes.count; ++q)
+      if (mhit::prepare_poisson(kSizes.n[q]) != cudaSuccess) return MHIT_ERR_CUDA;
+    t.ready = true;
+    a = t;
   }
   *out = a;
   return MHIT_OK;
-}
-
-bool built_size(int n) {
-  bool ok = false;
-#define MHIT_CASE(NN) ok |= (n == NN);
-  MHIT_FOR_SIZES(MHIT_CASE)
-#undef MHIT_CASE
-  return ok;
 }
 
 }  // namespace
@@ -75,49 +154,21 @@ extern "C" int mhit_poisson_noalloc(const double* rhs_dev, double* p_dev, int n,
                                     void* stream) {
   if (!rhs_dev || !p_dev || n < 2) return MHIT_ERR_INVALID;
   if (n > kMaxN) return MHIT_ERR_SCRATCH_LIMIT;
-  if (!built_size(n)) return MHIT_ERR_UNSUPPORTED;
+  const int slot = size_slot(n);
+  if (slot < 0) return MHIT_ERR_UNSUPPORTED;
+  if (mhit::spectrum_pitch(n, 0) > kPitchMax) return MHIT_ERR_SCRATCH_LIMIT;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return MHIT_ERR_CUDA;
   Addrs a;
   int rc = setup_device(dev, &a);
   if (rc) return rc;
-  if (mhit::spectrum_pitch(n, 0) > kPitchMax) return MHIT_ERR_SCRATCH_LIMIT;
-  if (mhit::prepare_poisson(n) != cudaSuccess) return MHIT_ERR_CUDA;
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-
-  // Tables on the host stack, as mhit_create builds them (same values, so the
-  // result equals mhit_poisson_device's bit for bit).
-  double2 tw[kMaxN];
-  double k2[kMaxN];
-  const double twopi = 8.0 * atan(1.0);
-  const double lx = twopi;
-  const double dx = (grid_mode == MHIT_GRID_CONSISTENT) ? lx / n : lx / (n - 1);
-  const double ddxi = 1.0 / dx / dx;
-  const double pi = 4.0 * atan(1.0);
-  for (int m = 0; m < n; ++m) {
-    long double ang = 2.0L * 3.141592653589793238462643383279502884L * (long double)m / (long double)n;
-    tw[m].x = (double)cosl(ang);
-    tw[m].y = -(double)sinl(ang);
-    if (k2_mode == MHIT_K2_FD) {
-      const double s = sin(pi * m / n);
-      k2[m] = (4.0 * ddxi) * (s * s);
-    } else {
-      const double kk = (m < n / 2 ? (double)m : (double)(m - n)) * (twopi / lx);
-      k2[m] = kk * kk;
-    }
-  }
-  // Pageable-source copies return once the source has been staged, so the
-  // stack arrays may go out of scope afterwards.
-  if (cudaMemcpyAsync(a.tw, tw, n * sizeof(double2), cudaMemcpyHostToDevice, st) != cudaSuccess) return MHIT_ERR_CUDA;
-  if (cudaMemcpyAsync(a.k2, k2, n * sizeof(double), cudaMemcpyHostToDevice, st) != cudaSuccess) return MHIT_ERR_CUDA;
-
   mhit::PoissonArgs<double> pa;
   pa.rhs = rhs_dev;
   pa.spec = a.spec;
   pa.p = p_dev;
-  pa.tw = a.tw;
-  pa.k2tab = a.k2;
+  pa.tw = a.tw + kSizes.off[slot];
+  pa.k2tab = a.k2 + (size_t)mode_index(k2_mode, grid_mode) * kSizes.total + kSizes.off[slot];
   pa.ctrl = nullptr;
-  if (mhit::launch_poisson<double>(n, pa, st) != cudaSuccess) return MHIT_ERR_CUDA;
+  if (mhit::launch_poisson<double>(n, pa, static_cast<cudaStream_t>(stream)) != cudaSuccess) return MHIT_ERR_CUDA;
   return MHIT_OK;
 }

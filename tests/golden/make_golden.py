@@ -5,14 +5,15 @@
    dissipation of the Taylor-Green vortex (nu = 6.25e-4, dt = 2e-4, rho = 1,
    no forcing, phase field off; val/comparison_diss.m:5,10) every 0.2 time
    units, i.e. every 1000 steps.  Read from the reference checkout given by
-   --reference (default /root/reference) and copied verbatim as numbers.
+   --reference (or the MHIT36_REFERENCE environment variable) and copied
+   verbatim as numbers.
 
 2. (with --oracle) oracle_taylor_green_128.json -- the CPU oracle's own
    dissipation on the same case at t = 0, 0.2, 0.4 (1000 and 2000 steps at
    128^3), recording how closely the oracle reproduces the reference's series.
    Takes a few minutes on 8 cores.
 
-    python tests/golden/make_golden.py [--reference DIR] [--oracle]
+    python tests/golden/make_golden.py --reference DIR [--oracle]
 """
 from __future__ import annotations
 
@@ -66,9 +67,12 @@ def oracle_check(steps=(1000, 2000)) -> dict:
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("MHIT36_REFERENCE"),
+                    help="checkout of aroccon/MHIT36 (or set MHIT36_REFERENCE)")
     ap.add_argument("--oracle", action="store_true")
     a = ap.parse_args()
+    if not a.reference:
+        ap.error("give the reference checkout with --reference DIR or MHIT36_REFERENCE")
     val = extract_val(a.reference)
     with open(os.path.join(HERE, "val_taylor_green.json"), "w") as f:
         json.dump(val, f, indent=1)

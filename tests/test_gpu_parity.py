@@ -235,15 +235,35 @@ def test_phi_volume_conserved_and_bounded():
     assert phi.min() > -0.05 and phi.max() < 1.05
 
 
-def test_ns_acdi_256_3_steps():
-    """256^3 NS+ACDI (8 drops) against the oracle: exercises the 8x8x4 radix
-    plan and the x inverse fused into the projection, whose pressure is
-    recomputed from the last step's spectrum on request."""
-    p = _params()
-    ref, got, od, d, pref, pgot = run_pair(256, 3, True, p)
-    _check(ref, got, True)
-    assert rel_err(pgot, pref) <= 1e-11
-    assert abs(d["umax"] - od["umax"]) <= 1e-12 * abs(od["umax"])
+def test_ns_acdi_256_10_steps_every_tile_shape():
+    """256^3 NS+ACDI (8 drops) for 10 steps against the oracle: exercises the
+    8x8x4 radix plan and the x inverse fused into the projection, whose
+    pressure is recomputed from the last step's spectrum on request.  The GPU
+    runs the default tiles and every (z chunk, momentum tile height) the
+    ensemble's autotuner may pick, each against the same oracle run."""
+    from oracle import Oracle
+    from mhit36_b200 import Solver
+    n, steps = 256, 10
+    p = _params(dt=5e-4)  # inside the explicit ACDI diffusion limit Umax*dt/dx < 1/6
+    case = _case(n, True)
+    o = Oracle(n, phase_field=1, **_oracle_kw(p))
+    o.set_fields(*case)
+    rc, od = o.step(steps)
+    assert rc == 0
+    ref = o.get_fields()
+    pref = o.get_pressure()
+    o.close()
+    for kz, mty in [(0, 0), (64, 8), (32, 16), (16, 8), (16, 16), (8, 8), (8, 16)]:
+        with Solver(n, p, phase_field=True) as s:
+            s.set_tiles(kz, mty)
+            s.set_fields(*case)
+            d = s.step(steps)
+            got = s.get_fields()
+            pgot = s.get_pressure()
+        errs = _check(ref, got, True)
+        assert rel_err(pgot, pref) <= 1e-11, (kz, mty)
+        assert abs(d["umax"] - od["umax"]) <= 1e-12 * abs(od["umax"]), (kz, mty, errs)
+        assert abs(d["cfl"] - od["cfl"]) <= 1e-12 * abs(od["cfl"]), (kz, mty)
 
 
 @pytest.mark.parametrize("n", [256, 512])
