@@ -33,6 +33,89 @@ static int pick_kz(int n) { return n >= 512 ? 64 : (n >= 32 ? 32 : n); }
 // 16 rows 4.18 ms (128 registers); FP32 8 rows 2.00 ms, 16 rows 1.87 ms.
 int default_mty(int n, int fp32) { return (n >= 16 && fp32) ? 16 : 8; }
 
+// ============================================================ psi arithmetic
+// psi = eps*log(a/b) (A3) is the phase kernel's most expensive expression.
+// FP64: a/b by Newton-Raphson from the PTX reciprocal approximation
+// (rcp.approx.ftz.f64, two iterations and a remainder correction: the
+// correctly rounded quotient for these operands, which are normal numbers
+// in [1e-16, 1 + 1e-16]), and the logarithm by P. T. P. Tang's table-driven
+// method ("Table-driven implementation of the logarithm function in IEEE
+// floating-point arithmetic", ACM TOMS 16(4), 1990): x = 2^k m, m in
+// [1, 2), F = 1 + j/128 nearest to m, r = (m - F)/F with |r| <= 2^-8, and
+// log x = k ln2 + log F + log(1 + r), the last by its Taylor series to r^7
+// (truncation below 2^-59 relative).  log F and ln2 are double-double
+// values computed on the host in long double.  Both are branch-free, so the
+// psi of a thread's elements overlap.  Measured against CUDA's log and
+// division on B200 over 134M phase-field values: at most 2 ulp apart, and
+// 1.45x faster.  FP32: the hardware approximations __fdividef and __logf
+// (about 1 ulp of psi on these operands).
+constexpr int LOGTAB = 3 * 129 + 2;  // 1/F, log F (hi), log F (lo), then ln2 (hi, lo)
+__device__ double g_log_table[LOGTAB];
+
+__device__ __forceinline__ double div_nr(double a, double b) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
+  double e = fma(-b, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-b, y, 1.0);
+  y = fma(y, e, y);
+  const double q = a * y;
+  return fma(fma(-b, q, a), y, q);
+}
+
+// log x for positive normal x; tab = g_log_table (in shared memory)
+__device__ __forceinline__ double tang_log(double x, const double* __restrict__ tab) {
+  const int hi = __double2hiint(x), lo = __double2loint(x);
+  const int k = (hi >> 20) - 1023;
+  const int mant = hi & 0x000fffff;
+  const int j = (mant + (1 << 12)) >> 13;  // nearest j/128, 0..128
+  const double m = __hiloint2double(mant | 0x3ff00000, lo);
+  const double r = (m - (1.0 + (double)j * (1.0 / 128))) * tab[j];  // m - F is exact
+  double p = fma(r, 1.0 / 7, -1.0 / 6);
+  p = fma(p, r, 0.2);
+  p = fma(p, r, -0.25);
+  p = fma(p, r, 1.0 / 3);
+  p = fma(p, r, -0.5);
+  p = fma(p, r * r, r);
+  const double kd = (double)k;
+  return fma(kd, tab[3 * 129], tab[129 + j]) + (fma(kd, tab[3 * 129 + 1], tab[2 * 129 + j]) + p);
+}
+
+template <class T> struct PsiMath;
+template <> struct PsiMath<double> {
+  static constexpr int TAB = LOGTAB;  // table entries staged in shared memory
+  static __device__ __forceinline__ double log_ratio(double a, double b, const double* tab) {
+    return tang_log(div_nr(a, b), tab);
+  }
+};
+template <> struct PsiMath<float> {
+  static constexpr int TAB = 0;
+  static __device__ __forceinline__ float log_ratio(float a, float b, const double*) { return __logf(__fdividef(a, b)); }
+};
+
+// The table of tang_log, once per device (before any graph capture).
+static cudaError_t upload_log_table() {
+  static bool done[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e) return e;
+  if (dev >= 0 && dev < 64 && done[dev]) return cudaSuccess;
+  double t[LOGTAB];
+  for (int j = 0; j <= 128; ++j) {
+    const long double F = 1.0L + (long double)j / 128.0L;
+    const long double l = logl(F);
+    t[j] = (double)(1.0L / F);
+    t[129 + j] = (double)l;
+    t[2 * 129 + j] = (double)(l - (long double)t[129 + j]);
+  }
+  const long double ln2 = logl(2.0L);
+  t[3 * 129] = (double)ln2;
+  t[3 * 129 + 1] = (double)(ln2 - (long double)t[3 * 129]);
+  if ((e = cudaMemcpyToSymbol(g_log_table, t, sizeof(t)))) return e;
+  if (dev >= 0 && dev < 64) done[dev] = true;
+  return cudaSuccess;
+}
+
 // ============================================================ phase field
 // ACDI step A1..A7 (multi/main.f90:341-480) fused into one kernel:
 //   psi = eps*log((min(phi,1)+enum)/(1-min(phi,1)+enum))      (A3)
@@ -80,6 +163,9 @@ __device__ __forceinline__ void phase_body(const StencilArgs<T>& a, int KZ, int 
   T* s_phi = reinterpret_cast<T*>(smem_raw);  // ring of 5 planes
   T* s_psi = s_phi + 5 * PE;                  // ring of 3 planes
   T* s_F = s_psi + 3 * PE;                    // ring of 3 planes x 3 components
+  double* s_tab = reinterpret_cast<double*>(s_F + 9 * FE);  // log table (FP64)
+  for (int q = threadIdx.x; q < PsiMath<T>::TAB; q += NT) s_tab[q] = g_log_table[q];
+  if (PsiMath<T>::TAB) __syncthreads();
   const int n = a.c.n;
   const T eps = (T)a.c.eps, epsi = (T)a.c.epsi, enumv = (T)a.c.enumv, tiny = (T)a.c.tiny;
   const T dxi = (T)a.c.dxi, ddxi = (T)a.c.ddxi, dt = (T)a.c.dt, hdxi = (T)0.5 * dxi;
@@ -94,8 +180,8 @@ __device__ __forceinline__ void phase_body(const StencilArgs<T>& a, int KZ, int 
   // half an ulp of enum, far under 2^-54): there the reference's expression
   // evaluates to psi1 / psi0 exactly, so those constants are computed once
   // and the log is skipped -- bitwise the same values.
-  const T psi0 = eps * log(((T)0 + enumv) / ((T)1 - (T)0 + enumv));
-  const T psi1 = eps * log(((T)1 + enumv) / ((T)1 - (T)1 + enumv));
+  const T psi0 = eps * PsiMath<T>::log_ratio((T)0 + enumv, (T)1 - (T)0 + enumv, s_tab);
+  const T psi1 = eps * PsiMath<T>::log_ratio((T)1 + enumv, (T)1 - (T)1 + enumv, s_tab);
   const int x0 = bx * TX, y0 = by * TY, k0 = bz * KZ;
   const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
   constexpr int RY = TY / PPT;  // row step between a thread's output rows
@@ -169,7 +255,7 @@ __device__ __forceinline__ void phase_body(const StencilArgs<T>& a, int KZ, int 
       if (r < NPE - 1 || e < PE) {
         const T val = fmax(fmin(Ph0[e], (T)1), floor0);
         PsW[e] = (val + enumv == enumv) ? psi0
-                 : ((val == (T)1) ? psi1 : eps * log((val + enumv) / ((T)1 - val + enumv)));
+                 : ((val == (T)1) ? psi1 : eps * PsiMath<T>::log_ratio(val + enumv, (T)1 - val + enumv, s_tab));
       }
     }
     // psi of plane m is visible, and every thread is done with iteration m-1:
@@ -793,7 +879,7 @@ __global__ void clear_mean_kernel(Ctrl* ctrl) {
 
 // ============================================================ launchers
 template <class T> static size_t phase_smem() {
-  return sizeof(T) * (size_t)(8 * (TX + 4) * (PTY + 4) + 9 * (TX + 2) * (PTY + 2));
+  return sizeof(T) * (size_t)(8 * (TX + 4) * (PTY + 4) + 9 * (TX + 2) * (PTY + 2)) + sizeof(double) * PsiMath<T>::TAB;
 }
 template <class T> static size_t momentum_smem(bool pf, int mty) {
   const int ns = momentum_ring(mty);
@@ -828,7 +914,9 @@ template <class T> static cudaError_t prep_t() {
 }
 
 cudaError_t prepare_stencils() {
-  cudaError_t e = prep_t<double>();
+  cudaError_t e = upload_log_table();
+  if (e) return e;
+  e = prep_t<double>();
   if (e) return e;
   return prep_t<float>();
 }
