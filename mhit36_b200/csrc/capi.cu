@@ -53,6 +53,13 @@ struct mhit_handle {
   // step; the spectrum still holds the last step's y-inverse output, from
   // which mhit_get_pressure recomputes p.
   bool p_in_spec = false;
+  // FP32 refinement form with the fused x inverse + projection: dp is not
+  // stored by the step; the spectrum holds the last correction solve's
+  // y-inverse output, from which dp (for the pressure and the divergence
+  // check) is recomputed on request.
+  bool dp_in_spec = false;
+  bool have_step = false;     // a step ran since the fields were set (ustar, p0 are its own)
+  double* div_out = nullptr;  // device: max |div u| of the FP64 projection (FP32 refine form)
   double* stat_partials = nullptr;
   double* stat_out = nullptr;
   double* h_stat = nullptr;  // pinned
@@ -222,15 +229,22 @@ std::vector<Stage> step_stages(mhit_handle* h, int cur) {
     mhit::PoissonArgs<float> pr = pa;
     pr.pres = h->fp0;  // residual r - L(p0) in FP64
     pr.p = h->fdp;
-    for (int k = 0; k < 5; ++k)
+    const bool fused = mhit::fused_projection(n) != 0;
+    for (int k = 0; k < (fused ? 4 : 5); ++k)
       v.push_back({rnames[k], [pr, n, k, st] { return mhit::launch_poisson_stage<float>(n, pr, k, st); }});
     float* dp = h->fdp;
-    v.push_back({"project", [a, dp, st] { return mhit::launch_project_refine(a, dp, st); }});
+    if (fused)
+      v.push_back({"xinvproj", [pr, a, n, st] { return mhit::launch_xinv_project<float>(n, pr, a, st); }});
+    else
+      v.push_back({"project", [a, dp, st] { return mhit::launch_project_refine(a, dp, st); }});
     Ctrl* ctrl = h->ctrl;
     double* part = h->partials;
     int np = h->nparts;
     StepConst c = h->c;
-    v.push_back({"finalize", [part, np, ctrl, c, st] { return mhit::launch_finalize(part, np, 7, ctrl, c, st); }});
+    const int stride = fused ? 6 : 7;
+    v.push_back({"finalize", [part, np, ctrl, c, st, stride] {
+                   return mhit::launch_finalize(part, np, stride, ctrl, c, st);
+                 }});
   }
   return v;
 }
@@ -383,6 +397,38 @@ cudaError_t pull_ctrl(mhit_handle* h) {
   return cudaStreamSynchronize(h->st);
 }
 
+bool refine_fused(mhit_handle* h) { return f32(h) && mhit::fused_projection(h->n); }
+
+// FP32 refinement form with the fused projection: dp = x inverse of the
+// last correction solve's spectrum, into the dp buffer.
+cudaError_t materialize_dp(mhit_handle* h) {
+  if (!h->dp_in_spec) return cudaSuccess;
+  mhit::PoissonArgs<float> pr;
+  pr.spec = h->fspec;
+  pr.p = h->fdp;
+  pr.tw = h->ftw;
+  pr.k2tab = h->k2tab;
+  pr.ctrl = nullptr;
+  cudaError_t e = mhit::launch_poisson_stage<float>(h->n, pr, 4, h->st);
+  if (!e) h->dp_in_spec = false;
+  return e;
+}
+
+// max |div u| of the last step's FP64 projection (FP32 refinement form),
+// measured from the stored ustar, p0 and dp; -1 before the first step.
+cudaError_t refine_max_div(mhit_handle* h, double* out) {
+  *out = h->h_ctrl->max_div;
+  if (!refine_fused(h) || !h->have_step) return cudaSuccess;
+  cudaError_t e = materialize_dp(h);
+  if (e) return e;
+  const int cur = (int)(h->h_ctrl->nstep & 1);
+  if ((e = mhit::launch_refine_divergence(stencil_args<float>(h, cur), h->fdp, h->div_out, h->st))) return e;
+  if ((e = cudaMemcpyAsync(h->h_stat, h->div_out, sizeof(double), cudaMemcpyDeviceToHost, h->st))) return e;
+  if ((e = cudaStreamSynchronize(h->st))) return e;
+  *out = h->h_stat[0];
+  return cudaSuccess;
+}
+
 }  // namespace
 
 extern "C" {
@@ -511,12 +557,13 @@ int mhit_create(const mhit_params* p, int nx, int ny, int nz, int precision, int
         break;
       }
     }
-    h->nparts = (precision == MHIT_FP64) ? mhit::step_partials_fp64(n) : mhit::project_partials(n);
+    h->nparts = mhit::fused_projection(n) ? mhit::xinv_project_partials(n) : mhit::project_partials(n);
     if ((e = dalloc(h, &h->partials, (size_t)mhit::partials_capacity(n) * 7 * sizeof(double)))) {
       fail(e, "cudaMalloc partials");
       break;
     }
     if ((e = dalloc(h, &h->ctrl, sizeof(Ctrl)))) { fail(e, "cudaMalloc ctrl"); break; }
+    if ((e = dalloc(h, &h->div_out, sizeof(double)))) { fail(e, "cudaMalloc div"); break; }
     if ((e = dalloc(h, &h->stat_partials, (size_t)mhit::stats_partials(n) * 8 * sizeof(double))) ||
         (e = dalloc(h, &h->stat_out, 8 * sizeof(double))) || (e = cudaMallocHost(&h->h_stat, 8 * sizeof(double)))) {
       fail(e, "cudaMalloc stats");
@@ -613,6 +660,8 @@ int mhit_set_fields(mhit_handle* h, const double* u, const double* v, const doub
     CK(h, cudaMemsetAsync(h->p, 0, fb, h->st));
     h->p_in_spec = false;
   }
+  h->dp_in_spec = false;
+  h->have_step = false;
   reset_ctrl(h);
   CK(h, cudaMemcpyAsync(h->ctrl, h->h_ctrl, sizeof(Ctrl), cudaMemcpyHostToDevice, h->st));
   CK(h, cudaStreamSynchronize(h->st));
@@ -653,6 +702,7 @@ int mhit_get_pressure(mhit_handle* h, double* p, int layout) {
   if (!h || !p || !layout_ok(layout)) return MHIT_ERR_INVALID;
   DeviceGuard g(h->device);
   if (f32(h)) {
+    CK(h, materialize_dp(h));
     const size_t N3 = (size_t)h->n * h->n * h->n;
     std::vector<double> a(N3), b(N3);
     CK(h, get_field(h, a.data(), DevField{h->fp0, true}, MHIT_LAYOUT_RAW));
@@ -691,10 +741,13 @@ int mhit_step(mhit_handle* h, int nsteps, mhit_diag* out) {
     CK(h, cudaGraphLaunch(h->graph[cur], h->st));
     ++h->nstep_host;
     h->p_in_spec = !f32(h) && mhit::fused_projection(h->n);
+    h->dp_in_spec = refine_fused(h);
+    h->have_step = true;
   }
   CK(h, pull_ctrl(h));
   h->nstep_host = h->h_ctrl->nstep;  // fewer if a step raised the error status
   fill_diag(h, out);
+  if (out) CK(h, refine_max_div(h, &out->max_div));
   return h->h_ctrl->status;
 }
 
@@ -709,6 +762,8 @@ int mhit_step_async(mhit_handle* h, int nsteps) {
     CK(h, cudaGraphLaunch(h->graph[cur], h->st));
     ++h->nstep_host;
     h->p_in_spec = !f32(h) && mhit::fused_projection(h->n);
+    h->dp_in_spec = refine_fused(h);
+    h->have_step = true;
   }
   return MHIT_OK;
 }
@@ -719,6 +774,7 @@ int mhit_get_diag(mhit_handle* h, mhit_diag* out) {
   CK(h, pull_ctrl(h));
   h->nstep_host = h->h_ctrl->nstep;
   fill_diag(h, out);
+  CK(h, refine_max_div(h, &out->max_div));
   return MHIT_OK;
 }
 
@@ -865,6 +921,8 @@ int mhit_profile_step(mhit_handle* h, int reps, double* ms, int* nstages) {
     }
     CK(h, cudaEventSynchronize(ev[NS]));
     h->p_in_spec = !f32(h) && mhit::fused_projection(h->n);
+    h->dp_in_spec = refine_fused(h);
+    h->have_step = true;
     for (int i = 0; i < NS; ++i) {
       float t = 0;
       CK(h, cudaEventElapsedTime(&t, ev[i], ev[i + 1]));
@@ -1055,6 +1113,7 @@ int mhit_load(mhit_handle* h, const char* dir, int t) {
   CK(h, cudaMemcpyAsync(h->ctrl, c, sizeof(Ctrl), cudaMemcpyHostToDevice, h->st));
   CK(h, cudaStreamSynchronize(h->st));
   h->nstep_host = sc.nstep;
+  h->have_step = false;
   return MHIT_OK;
 }
 

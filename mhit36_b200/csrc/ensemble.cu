@@ -506,7 +506,7 @@ cudaError_t enqueue_class_step(Class* c, int kz, int mty) {
     for (int k = 0; k < (fused ? 4 : 5); ++k)
       if ((err = mhit::launch_poisson_stage_batched<double>(t, S, n, k, 0, c->st))) return err;
     if (fused) {
-      if ((err = mhit::launch_xinv_project_batched(t, S, n, c->st))) return err;
+      if ((err = mhit::launch_xinv_project_batched<double>(t, S, n, c->st))) return err;
     } else if ((err = mhit::launch_project_batched<double>(t, S, n, c->st))) {
       return err;
     }
@@ -515,10 +515,17 @@ cudaError_t enqueue_class_step(Class* c, int kz, int mty) {
   const SlotArgs<float>* t = static_cast<const SlotArgs<float>*>(c->d_slots);
   if (c->pf && (err = mhit::launch_phase_batched<float>(t, S, n, kz, c->st))) return err;
   if ((err = mhit::launch_momentum_batched<float>(t, S, n, kz, c->pf != 0, c->st, mty))) return err;
+  // first solve -> p0; correction solve of the FP64 residual, whose x inverse
+  // is fused into the projection where the size allows
+  const bool fused = mhit::fused_projection(n) != 0;
   for (int w = 0; w < 2; ++w)
-    for (int k = 0; k < 5; ++k)
+    for (int k = 0; k < ((w && fused) ? 4 : 5); ++k)
       if ((err = mhit::launch_poisson_stage_batched<float>(t, S, n, k, w, c->st))) return err;
-  if ((err = mhit::launch_project_batched<float>(t, S, n, c->st))) return err;
+  if (fused) {
+    if ((err = mhit::launch_xinv_project_batched<float>(t, S, n, c->st))) return err;
+  } else if ((err = mhit::launch_project_batched<float>(t, S, n, c->st))) {
+    return err;
+  }
   return mhit::launch_finalize_batched_f32(t, S, n, c->st);
 }
 

@@ -96,12 +96,21 @@ template <class T> cudaError_t launch_materialize(T* u, T* v, T* w, int n, Ctrl*
 cudaError_t prepare_stencils();
 int project_partials(int n);
 int stencil_size_ok(int n);
-// FP64 step with the x inverse fused into the projection (power-of-two
-// n >= 256): one kernel after the y inverse pass, writing its own partials.
+// The x inverse fused into the projection (power-of-two n >= 256): one
+// kernel after the y inverse pass, writing its own partials (stride 6).
+// FP64 step: pa is the solve; FP32 refinement form: pa is the correction
+// solve, whose x inverse dp is added to the stored p0 (a.p).
 int fused_projection(int n);
 int xinv_project_partials(int n);
-cudaError_t launch_xinv_project(int n, const PoissonArgs<double>& pa, const StencilArgs<double>& a, cudaStream_t st);
-cudaError_t launch_xinv_project_batched(const SlotArgs<double>* slots, int nslots, int n, cudaStream_t st);
+template <class T>
+cudaError_t launch_xinv_project(int n, const PoissonArgs<T>& pa, const StencilArgs<T>& a, cudaStream_t st);
+template <class T>
+cudaError_t launch_xinv_project_batched(const SlotArgs<T>* slots, int nslots, int n, cudaStream_t st);
+// FP32 refinement form: max |div u| of the FP64 projection u = ustar -
+// dt/rho*grad(p0 + dp) from the stored ustar, p0 and dp, into *out (one
+// double on the device; the forward-difference divergence of
+// multi/main.f90:723-725).
+cudaError_t launch_refine_divergence(const StencilArgs<float>& a, const float* dp, double* out, cudaStream_t st);
 // Partials the FP64 step's projection writes, and the buffer size that
 // holds either projection's partials (stride 7).
 inline int step_partials_fp64(int n) { return fused_projection(n) ? xinv_project_partials(n) : project_partials(n); }

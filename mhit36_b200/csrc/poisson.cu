@@ -135,6 +135,26 @@ struct ColSlab {
   bool live;         // false: skip (inactive slot or stopped simulation)
 };
 
+// The z solve's per-mode factor -1/(k^2 nx ny nz) (multi/main.f90:792), for
+// d = k^2 nx ny nz > 0.  FP64: the quotient by Newton-Raphson from the PTX
+// reciprocal approximation (rcp.approx.ftz.f64, two iterations and a
+// remainder correction; branch-free, unlike the IEEE division with its
+// special-case path), applied in FP64.  FP32 solves (the refinement form):
+// the single-precision reciprocal, whose relative error (about 1e-7) is of
+// the order of the FP32 transform's own rounding, which the FP64 residual
+// and correction solve remove.
+template <class T> __device__ __forceinline__ T scale_factor(double d);
+template <> __device__ __forceinline__ double scale_factor<double>(double d) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(d));
+  double e = fma(-d, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-d, y, 1.0);
+  y = fma(y, e, y);
+  return -fma(fma(-d, y, 1.0), y, y);
+}
+template <> __device__ __forceinline__ float scale_factor<float>(double d) { return -__frcp_rn((float)d); }
+
 template <int N, int KIND, class T>
 __device__ __forceinline__ void colpass_issue(typename C2<T>::t* buf, const ColSlab& sl) {
   typedef typename C2<T>::t C;
@@ -175,9 +195,9 @@ __device__ __forceinline__ void colpass_compute(typename C2<T>::t* s, const ColS
         v.y = 0;
       } else {
         const double k2 = (k2tab[m] + k2y) + k2tab[n];
-        const double f = -1.0 / (k2 * nnn);
-        v.x = (T)((double)v.x * f);
-        v.y = (T)((double)v.y * f);
+        const T f = scale_factor<T>(k2 * nnn);
+        v.x = v.x * f;
+        v.y = v.y * f;
       }
       return v;
     });
@@ -391,9 +411,9 @@ __device__ __forceinline__ void rcol_run(int total, const typename C2<T>::t* __r
           v[m].y = 0;
         } else {
           const double k2 = k2xy + k2tab[n];
-          const double f = -1.0 / (k2 * nnn);
-          v[m].x = (T)((double)v[m].x * f);
-          v[m].y = (T)((double)v[m].y * f);
+          const T f = scale_factor<T>(k2 * nnn);
+          v[m].x = v[m].x * f;
+          v[m].y = v[m].y * f;
         }
       }
       reg_fft_stages<N, 1, +1>(v, s, tw, t, at);
@@ -627,42 +647,54 @@ __device__ __forceinline__ void xfwd_reg_body(const T* __restrict__ us, const T*
 }
 
 // ---------------------------------------------------------------- x inverse fused with the projection
-// FP64 step, power-of-two N >= 256 (C2 + R1 of multi/main.f90:812-903 in one
-// pass): p never goes to HBM.  A CTA owns the output rows j0 .. j0+2P-1 of
+// Power-of-two N >= 256 (C2 + R1 of multi/main.f90:812-903 in one pass): the
+// pressure never goes to HBM.  A CTA owns the output rows j0 .. j0+2P-1 of
 // a chunk of KZ planes and marches through them.  Per plane it runs the x
 // inverse of its P line pairs plus one halo pair below (rows j0-2, j0-1;
 // the projection's backward difference in y needs row j0-1), puts the
-// plane's p rows into shared memory, and projects the plane:
+// plane's pressure rows into shared memory, and projects the plane:
 //   u = ustar - dt/rho*(p - p(i-1))*dxi, v with p(j-1), w with p(k-1),
 // where p(k-1) is the previous plane's rows, kept in a second buffer (the
 // chunk starts one plane early to fill it).  Per-CTA FP64 sums and maxima
-// as in project_body, in a fixed order.  The x inverse is xinv_reg_body's
-// arithmetic and the projection project_body's, so u, v, w and the
-// pressure (recomputed from the spectrum on request) are the same bits as
-// the unfused kernels give; only the grouping of the sums that make the
-// means differs.  Traffic per point: the half spectrum (8.06 B, plus the
-// halo rows, mostly L2 hits) + ustar, vstar, wstar + u, v, w: the 280 B/pt
-// schedule instead of 296.
-template <int N> struct XPCfg {
-  static constexpr bool ON = RCfg<N, double>::ON && N >= 256;
-  static constexpr int P = PCfg<N, double>::P;
+// as in project_body, in a fixed order.
+//   * FP64 step (T = double): p is the x inverse of the spectrum.  The x
+//     inverse is xinv_reg_body's arithmetic and the projection
+//     project_body's, so u, v, w and the pressure (recomputed from the
+//     spectrum on request) are the same bits as the unfused kernels give;
+//     only the grouping of the sums that make the means differs.  Traffic
+//     per point: the half spectrum (8.06 B, plus the halo rows, mostly L2
+//     hits) + ustar, vstar, wstar + u, v, w: the 280 B/pt schedule instead
+//     of 296.
+//   * FP32 refinement form (T = float): the spectrum is the correction
+//     solve's; its x inverse is dp, and the pressure p = p0 + dp is formed
+//     in FP64 from the first solve's stored p0.  The projection runs in FP64
+//     and rounds u, v, w to FP32 when storing them (project_refine_body's
+//     arithmetic, without its forward-difference divergence, which
+//     refine_divergence measures on request from the same stored inputs).
+//     dp never goes to HBM: 32 B/pt instead of the 40 of the separate x
+//     inverse and projection.
+template <int N, class T> struct XPCfg {
+  static constexpr bool ON = RCfg<N, T>::ON && N >= 256;
+  static constexpr int P = PCfg<N, T>::P;
   static constexpr int TPC = N / 8;
   static constexpr int NT = (P + 1) * TPC;  // a multiple of 32 for N >= 256
   static constexpr int KZ = N >= 512 ? 16 : 8;
-  static constexpr size_t XBYTES = (size_t)(P + 1) * reg_rows(N) * sizeof(double2);  // exchange
-  static constexpr size_t PBYTES = (size_t)(2 * P + 1) * N * sizeof(double);         // plane's p rows
-  static constexpr size_t ABYTES = XBYTES > PBYTES ? XBYTES : PBYTES;                // the two alias
-  static constexpr size_t SMEM = ABYTES + (size_t)2 * P * N * sizeof(double);        // + previous plane
+  static constexpr size_t XBYTES = (size_t)(P + 1) * XCfg<N, T>::LS * sizeof(typename C2<T>::t);  // exchange
+  static constexpr size_t PBYTES = (size_t)(2 * P + 1) * N * sizeof(double);  // plane's p rows
+  static constexpr size_t ABYTES = XBYTES > PBYTES ? XBYTES : PBYTES;        // the two alias
+  static constexpr size_t SMEM = ABYTES + (size_t)2 * P * N * sizeof(double);  // + previous plane
   static constexpr int PARTS = (N / (2 * P)) * (N / KZ);
 };
 
-template <int N>
-__device__ __forceinline__ void xinvproj_body(const double2* __restrict__ spec, const double2* __restrict__ tw,
-                                              const StencilArgs<double>& a, int bx, int bz, int gx) {
-  typedef double2 C;
-  typedef XPCfg<N> X;
-  constexpr int P = X::P, TPC = X::TPC, NT = X::NT, KZ = X::KZ, RS = reg_rows(N);
-  constexpr size_t PITCH = PCfg<N, double>::PITCH;
+template <int N, class T>
+__device__ __forceinline__ void xinvproj_body(const typename C2<T>::t* __restrict__ spec,
+                                              const typename C2<T>::t* __restrict__ tw, const StencilArgs<T>& a,
+                                              int bx, int bz, int gx) {
+  typedef typename C2<T>::t C;
+  typedef XPCfg<N, T> X;
+  constexpr bool REF = sizeof(T) == 4;  // FP32 refinement form: p = p0 + dp
+  constexpr int P = X::P, TPC = X::TPC, NT = X::NT, KZ = X::KZ;
+  constexpr size_t PITCH = PCfg<N, T>::PITCH;
   static_assert(NT % 32 == 0, "whole warps");
   if (a.ctrl->status) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -674,18 +706,18 @@ __device__ __forceinline__ void xinvproj_body(const double2* __restrict__ spec, 
   const int ja = (q < P) ? j0 + 2 * q : (j0 - 2 + N) % N;
   const double dtr = a.c.dtr, dxi = a.c.dxi;
   const size_t nn = (size_t)N * N;
-  const double* __restrict__ us = a.us;
-  const double* __restrict__ vs = a.vs;
-  const double* __restrict__ ws = a.ws;
-  double* __restrict__ uo_ = a.uo;
-  double* __restrict__ vo_ = a.vo;
-  double* __restrict__ wo_ = a.wo;
+  const T* __restrict__ us = a.us;
+  const T* __restrict__ vs = a.vs;
+  const T* __restrict__ ws = a.ws;
+  T* __restrict__ uo_ = a.uo;
+  T* __restrict__ vo_ = a.vo;
+  T* __restrict__ wo_ = a.wo;
   constexpr int PIT = (2 * P * N + NT - 1) / NT;  // projection points per thread and plane
   constexpr int PG = 4;
   double su = 0, sv = 0, sw = 0;
   double xu = -INFINITY, xv = -INFINITY, xw = -INFINITY;
-  const int base = q * RS;
-  const auto at = [base](int n) { return base + reg_pad(n); };
+  const int base = q * XCfg<N, T>::LS;
+  const auto at = [base](int n) { return base + XCfg<N, T>::slot(n); };
   for (int kk = k0 - 1; kk < k0 + KZ; ++kk) {
     const int kw = (kk + N) % N;
     // (1) x inverse of the plane's line pairs (xinv_reg_body)
@@ -697,6 +729,17 @@ __device__ __forceinline__ void xinvproj_body(const double2* __restrict__ spec, 
       const int h = (n <= N / 2) ? n : N - n;
       A[m] = row[h];
       B[m] = row[PITCH + h];
+    }
+    // FP32 refinement form: the first solve's p0 on the same two rows
+    T pa0[8], pb0[8];
+    if constexpr (REF) {
+      const T* __restrict__ p0 = a.p;
+#pragma unroll
+      for (int m = 0; m < 8; ++m) {
+        const size_t g = (size_t)(t + TPC * m) + (size_t)N * ja + nn * kw;
+        pa0[m] = (q < P) ? p0[g] : (T)0;
+        pb0[m] = p0[g + N];
+      }
     }
     C v[8];
 #pragma unroll
@@ -721,11 +764,21 @@ __device__ __forceinline__ void xinvproj_body(const double2* __restrict__ spec, 
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
       const int n = t + TPC * m;
-      if (q < P) {
-        sp[(2 * q + 1) * N + n] = v[m].x;
-        sp[(2 * q + 2) * N + n] = v[m].y;
+      if constexpr (REF) {
+        const double pa = (double)pa0[m] + (double)v[m].x, pb = (double)pb0[m] + (double)v[m].y;
+        if (q < P) {
+          sp[(2 * q + 1) * N + n] = pa;
+          sp[(2 * q + 2) * N + n] = pb;
+        } else {
+          sp[n] = pb;
+        }
       } else {
-        sp[n] = v[m].y;
+        if (q < P) {
+          sp[(2 * q + 1) * N + n] = v[m].x;
+          sp[(2 * q + 2) * N + n] = v[m].y;
+        } else {
+          sp[n] = v[m].y;
+        }
       }
     }
     __syncthreads();
@@ -737,7 +790,7 @@ __device__ __forceinline__ void xinvproj_body(const double2* __restrict__ spec, 
     if (kk >= k0) {
 #pragma unroll 1
       for (int it0 = 0; it0 < PIT; it0 += PG) {
-        double lu[PG], lv[PG], lw[PG];
+        T lu[PG], lv[PG], lw[PG];
 #pragma unroll
         for (int c = 0; c < PG; ++c) {
           const int pi = threadIdx.x + NT * (it0 + c);
@@ -759,12 +812,12 @@ __device__ __forceinline__ void xinvproj_body(const double2* __restrict__ spec, 
             const double pym = sp[r * N + x];
             const double pzm = spp[r * N + x];
             const size_t g = (size_t)x + (size_t)N * (j0 + r) + nn * kw;
-            const double uo = lu[c] - dtr * (pc - pxm) * dxi;
-            const double vo = lv[c] - dtr * (pc - pym) * dxi;
-            const double wo = lw[c] - dtr * (pc - pzm) * dxi;
-            uo_[g] = uo;
-            vo_[g] = vo;
-            wo_[g] = wo;
+            const double uo = (double)lu[c] - dtr * (pc - pxm) * dxi;
+            const double vo = (double)lv[c] - dtr * (pc - pym) * dxi;
+            const double wo = (double)lw[c] - dtr * (pc - pzm) * dxi;
+            uo_[g] = (T)uo;
+            vo_[g] = (T)vo;
+            wo_[g] = (T)wo;
             su += uo;
             sv += vo;
             sw += wo;
@@ -811,20 +864,22 @@ __device__ __forceinline__ void xinvproj_body(const double2* __restrict__ spec, 
   }
 }
 
-template <int N>
-__global__ void __launch_bounds__(XPCfg<N>::NT, 2) xinvproj_kernel(const double2* __restrict__ spec,
-                                                                   const double2* __restrict__ tw,
-                                                                   StencilArgs<double> a) {
-  if constexpr (XPCfg<N>::ON) xinvproj_body<N>(spec, tw, a, blockIdx.x, blockIdx.y, gridDim.x);
+template <int N, class T>
+__global__ void __launch_bounds__(XPCfg<N, T>::NT, 2) xinvproj_kernel(const typename C2<T>::t* __restrict__ spec,
+                                                                      const typename C2<T>::t* __restrict__ tw,
+                                                                      StencilArgs<T> a) {
+  if constexpr (XPCfg<N, T>::ON) xinvproj_body<N, T>(spec, tw, a, blockIdx.x, blockIdx.y, gridDim.x);
 }
-template <int N>
-__global__ void __launch_bounds__(XPCfg<N>::NT, 2) xinvproj_kernel_b(const SlotArgs<double>* __restrict__ slots,
-                                                                     int zch) {
-  if constexpr (XPCfg<N>::ON) {
+// Batched: the FP64 step transforms the slot's spectrum, the FP32
+// refinement form its correction spectrum.
+template <int N, class T>
+__global__ void __launch_bounds__(XPCfg<N, T>::NT, 2) xinvproj_kernel_b(const SlotArgs<T>* __restrict__ slots,
+                                                                        int zch) {
+  if constexpr (XPCfg<N, T>::ON) {
     const int sl = blockIdx.y / zch;
     if (!slots[sl].active) return;
-    xinvproj_body<N>(slots[sl].po.spec, slots[sl].po.tw, slots[sl].st, blockIdx.x, blockIdx.y - sl * zch,
-                     gridDim.x);
+    const PoissonArgs<T>& pa = (sizeof(T) == 4) ? slots[sl].pr : slots[sl].po;
+    xinvproj_body<N, T>(pa.spec, pa.tw, slots[sl].st, blockIdx.x, blockIdx.y - sl * zch, gridDim.x);
   }
 }
 
@@ -968,10 +1023,11 @@ template <int N, class T> static cudaError_t set_attrs() {
     if ((e = cudaFuncSetAttribute(rcol_kernel_b<N, 1, T>, A, r1))) return e;
     if ((e = cudaFuncSetAttribute(rcol_kernel_b<N, 2, T>, A, r2))) return e;
   }
-  if constexpr (sizeof(T) == 8 && XPCfg<N>::ON) {
-    const int xs2 = (int)XPCfg<N>::SMEM;
-    if ((e = cudaFuncSetAttribute(xinvproj_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, xs2))) return e;
-    if ((e = cudaFuncSetAttribute(xinvproj_kernel_b<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, xs2))) return e;
+  if constexpr (XPCfg<N, T>::ON) {
+    const int xs2 = (int)XPCfg<N, T>::SMEM;
+    if ((e = cudaFuncSetAttribute(xinvproj_kernel<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, xs2))) return e;
+    if ((e = cudaFuncSetAttribute(xinvproj_kernel_b<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, xs2)))
+      return e;
   }
   return cudaSuccess;
 }
@@ -1005,20 +1061,20 @@ static cudaError_t poisson_run(const PoissonArgs<T>& a, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-template <int N>
-static cudaError_t xinvproj_run(const PoissonArgs<double>& pa, const StencilArgs<double>& a, cudaStream_t st) {
-  if constexpr (XPCfg<N>::ON) {
-    const dim3 grid(N / (2 * XPCfg<N>::P), N / XPCfg<N>::KZ);
-    xinvproj_kernel<N><<<grid, XPCfg<N>::NT, XPCfg<N>::SMEM, st>>>(pa.spec, pa.tw, a);
+template <int N, class T>
+static cudaError_t xinvproj_run(const PoissonArgs<T>& pa, const StencilArgs<T>& a, cudaStream_t st) {
+  if constexpr (XPCfg<N, T>::ON) {
+    const dim3 grid(N / (2 * XPCfg<N, T>::P), N / XPCfg<N, T>::KZ);
+    xinvproj_kernel<N, T><<<grid, XPCfg<N, T>::NT, XPCfg<N, T>::SMEM, st>>>(pa.spec, pa.tw, a);
     return cudaGetLastError();
   }
   return cudaErrorInvalidValue;
 }
-template <int N>
-static cudaError_t xinvproj_run_b(const SlotArgs<double>* slots, int nslots, cudaStream_t st) {
-  if constexpr (XPCfg<N>::ON) {
-    const dim3 grid(N / (2 * XPCfg<N>::P), (N / XPCfg<N>::KZ) * nslots);
-    xinvproj_kernel_b<N><<<grid, XPCfg<N>::NT, XPCfg<N>::SMEM, st>>>(slots, N / XPCfg<N>::KZ);
+template <int N, class T>
+static cudaError_t xinvproj_run_b(const SlotArgs<T>* slots, int nslots, cudaStream_t st) {
+  if constexpr (XPCfg<N, T>::ON) {
+    const dim3 grid(N / (2 * XPCfg<N, T>::P), (N / XPCfg<N, T>::KZ) * nslots);
+    xinvproj_kernel_b<N, T><<<grid, XPCfg<N, T>::NT, XPCfg<N, T>::SMEM, st>>>(slots, N / XPCfg<N, T>::KZ);
     return cudaGetLastError();
   }
   return cudaErrorInvalidValue;
@@ -1122,35 +1178,43 @@ cudaError_t launch_poisson(int n, const PoissonArgs<T>& a, cudaStream_t st) {
   }
 }
 
-cudaError_t launch_xinv_project(int n, const PoissonArgs<double>& pa, const StencilArgs<double>& a, cudaStream_t st) {
+template <class T>
+cudaError_t launch_xinv_project(int n, const PoissonArgs<T>& pa, const StencilArgs<T>& a, cudaStream_t st) {
   switch (n) {
 #define MHIT_CASE(NN) \
   case NN:            \
-    return xinvproj_run<NN>(pa, a, st);
+    return xinvproj_run<NN, T>(pa, a, st);
     MHIT_FOR_SIZES(MHIT_CASE)
 #undef MHIT_CASE
     default:
       return cudaErrorInvalidValue;
   }
 }
+template cudaError_t launch_xinv_project<double>(int, const PoissonArgs<double>&, const StencilArgs<double>&,
+                                                 cudaStream_t);
+template cudaError_t launch_xinv_project<float>(int, const PoissonArgs<float>&, const StencilArgs<float>&,
+                                                cudaStream_t);
 
-cudaError_t launch_xinv_project_batched(const SlotArgs<double>* slots, int nslots, int n, cudaStream_t st) {
+template <class T>
+cudaError_t launch_xinv_project_batched(const SlotArgs<T>* slots, int nslots, int n, cudaStream_t st) {
   switch (n) {
 #define MHIT_CASE(NN) \
   case NN:            \
-    return xinvproj_run_b<NN>(slots, nslots, st);
+    return xinvproj_run_b<NN, T>(slots, nslots, st);
     MHIT_FOR_SIZES(MHIT_CASE)
 #undef MHIT_CASE
     default:
       return cudaErrorInvalidValue;
   }
 }
+template cudaError_t launch_xinv_project_batched<double>(const SlotArgs<double>*, int, int, cudaStream_t);
+template cudaError_t launch_xinv_project_batched<float>(const SlotArgs<float>*, int, int, cudaStream_t);
 
 int fused_projection(int n) {
   switch (n) {
 #define MHIT_CASE(NN) \
   case NN:            \
-    return XPCfg<NN>::ON ? 1 : 0;
+    return (XPCfg<NN, double>::ON && XPCfg<NN, float>::ON) ? 1 : 0;
     MHIT_FOR_SIZES(MHIT_CASE)
 #undef MHIT_CASE
     default:
@@ -1162,7 +1226,7 @@ int xinv_project_partials(int n) {
   switch (n) {
 #define MHIT_CASE(NN) \
   case NN:            \
-    return XPCfg<NN>::ON ? XPCfg<NN>::PARTS : 0;
+    return XPCfg<NN, double>::ON ? XPCfg<NN, double>::PARTS : 0;
     MHIT_FOR_SIZES(MHIT_CASE)
 #undef MHIT_CASE
     default:

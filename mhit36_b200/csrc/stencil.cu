@@ -132,6 +132,9 @@ static cudaError_t upload_log_table() {
 constexpr int PTY = 16;            // phase tile height
 constexpr int PPT = 2;             // output rows per thread (rows ty + h*PTY/PPT)
 constexpr int PNT = TX * PTY / PPT;  // phase threads per CTA
+// Resident CTAs per SM the phase kernel is built for: 2 in FP64 (its FP64
+// registers), 4 in FP32 (64 registers; 512^3: 1.57 -> 1.37 ms against 2).
+template <class T> __host__ __device__ constexpr int phase_min_blocks() { return sizeof(T) == 4 ? 4 : 2; }
 
 // Momentum ring depth (planes per field): planes m-2 .. m+1, one in flight.
 // (A 5-plane ring with two planes in flight measured 30% slower on B200 at
@@ -738,6 +741,65 @@ __device__ __forceinline__ void project_refine_body(const StencilArgs<float>& a,
   }
 }
 
+// ============================================================ divergence check (FP32 refine)
+// On request, the max |div u| of the FP32 refinement form's FP64 projection
+// u = ustar - dt/rho*(p - p_m)*dxi with p = p0 + dp, from the stored ustar,
+// p0 and dp: the arithmetic of project_refine_body's divergence, so it
+// measures the field the step projected before rounding it to FP32.  Maxima
+// are order-independent: CTAs combine theirs with an integer atomicMax on the
+// bit patterns of the (non-negative, or NaN) values.
+__global__ void __launch_bounds__(NT) refine_div_kernel(StencilArgs<float> a, const float* __restrict__ dp,
+                                                        unsigned long long* __restrict__ out) {
+  const int n = a.c.n;
+  const double dtr = a.c.dtr, dxi = a.c.dxi;
+  const int i = blockIdx.x * TX + threadIdx.x % TX, j = blockIdx.y * TY + threadIdx.x / TX;
+  const int pkz = project_kz(n), k0 = blockIdx.z * pkz;
+  const int im = i ? i - 1 : n - 1, jm = j ? j - 1 : n - 1;
+  const int ip = (i + 1 == n) ? 0 : i + 1, jp = (j + 1 == n) ? 0 : j + 1;
+  const size_t nn = (size_t)n * n;
+  const float* p0 = a.p;
+  auto P = [&](size_t g) { return (double)p0[g] + (double)dp[g]; };
+  double mdiv = 0;
+  const size_t col = (size_t)i + (size_t)n * j;
+  double pm = P(col + nn * wrapi(k0 - 1, n));
+  double pc = P(col + nn * k0);
+  double wsc = (double)a.ws[col + nn * k0];
+  for (int k = k0; k < k0 + pkz; ++k) {
+    const size_t g = col + nn * k;
+    const size_t gzp = col + nn * ((k + 1 == n) ? 0 : k + 1);
+    const double pn = P(gzp);
+    const double wsn = (double)a.ws[gzp];
+    const size_t gxm = g - i + im, gxp = g - i + ip;
+    const size_t gym = g - (size_t)n * j + (size_t)n * jm, gyp = g - (size_t)n * j + (size_t)n * jp;
+    const double uo = (double)a.us[g] - dtr * (pc - P(gxm)) * dxi;
+    const double vo = (double)a.vs[g] - dtr * (pc - P(gym)) * dxi;
+    const double wo = wsc - dtr * (pc - pm) * dxi;
+    const double u1 = (double)a.us[gxp] - dtr * (P(gxp) - pc) * dxi;
+    const double v1 = (double)a.vs[gyp] - dtr * (P(gyp) - pc) * dxi;
+    const double w1 = wsn - dtr * (pn - pc) * dxi;
+    const double div = ((u1 - uo) + (v1 - vo) + (w1 - wo)) * dxi;
+    mdiv = fmax(mdiv, fabs(div));
+    if (div != div) mdiv = NAN;
+    pm = pc;
+    pc = pn;
+    wsc = wsn;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const double x = __shfl_xor_sync(0xffffffffu, mdiv, o);
+    mdiv = (x != x) ? x : fmax(mdiv, x);
+  }
+  if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(fabs(mdiv)));
+}
+
+cudaError_t launch_refine_divergence(const StencilArgs<float>& a, const float* dp, double* out, cudaStream_t st) {
+  const int n = a.c.n;
+  cudaError_t e = cudaMemsetAsync(out, 0, sizeof(double), st);
+  if (e) return e;
+  dim3 grid(n / TX, n / TY, n / project_kz(n));
+  refine_div_kernel<<<grid, NT, 0, st>>>(a, dp, reinterpret_cast<unsigned long long*>(out));
+  return cudaGetLastError();
+}
+
 // ============================================================ finalize
 // M1, C3, R2 and the CFL guard (multi/main.f90:906-946), one CTA:
 // means = sum/nx/ny/nz, removed lazily (stored in ctrl->mean and subtracted by
@@ -800,7 +862,7 @@ __device__ __forceinline__ void finalize_body(const double* __restrict__ partial
 // ============================================================ entry points
 // Single simulation: block coordinates are the grid's.
 template <class T>
-__global__ void __launch_bounds__(PNT, 2) phase_kernel(StencilArgs<T> a, int KZ) {
+__global__ void __launch_bounds__(PNT, phase_min_blocks<T>()) phase_kernel(StencilArgs<T> a, int KZ) {
   phase_body<T>(a, KZ, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 template <class T, bool PF, int MTYv>
@@ -823,7 +885,8 @@ __global__ void __launch_bounds__(FNT) finalize_kernel(const double* __restrict_
 // covers the slots; each slot runs exactly the arithmetic of a single
 // simulation, so a result is the same alone and in any mix.
 template <class T>
-__global__ void __launch_bounds__(PNT, 2) phase_kernel_b(const SlotArgs<T>* __restrict__ slots, int KZ, int zch) {
+__global__ void __launch_bounds__(PNT, phase_min_blocks<T>()) phase_kernel_b(const SlotArgs<T>* __restrict__ slots, int KZ,
+                                                                            int zch) {
   const int sl = blockIdx.z / zch;
   if (!slots[sl].active) return;
   StencilArgs<T> a = slots[sl].st;
@@ -1021,7 +1084,10 @@ cudaError_t launch_finalize_batched(const SlotArgs<double>* slots, int nslots, i
   return cudaGetLastError();
 }
 cudaError_t launch_finalize_batched_f32(const SlotArgs<float>* slots, int nslots, int n, cudaStream_t st) {
-  finalize_kernel_b<float><<<nslots, FNT, 0, st>>>(slots, project_partials(n), 7);
+  if (fused_projection(n))  // fused x inverse + projection: 6 values per CTA, no divergence
+    finalize_kernel_b<float><<<nslots, FNT, 0, st>>>(slots, xinv_project_partials(n), 6);
+  else
+    finalize_kernel_b<float><<<nslots, FNT, 0, st>>>(slots, project_partials(n), 7);
   return cudaGetLastError();
 }
 template cudaError_t launch_phase_batched<double>(const SlotArgs<double>*, int, int, int, cudaStream_t);

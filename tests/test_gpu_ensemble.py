@@ -149,3 +149,16 @@ def test_cancel():
         c = ens.submit(32, _params(), *case, nsteps=3)
         ens.run()
         _same(ens.result(c), _solo(32, _params(), case, 3))
+
+
+def test_fp32_fused_projection_class_matches_solver_bitwise():
+    """From 256^3 the FP32 refinement form fuses the correction solve's x
+    inverse into the projection, batched as in the plain Solver."""
+    from mhit36_b200.ensemble import Ensemble
+    p = _params(dt=2e-4, k2_mode=1)
+    case = _case(256, True, 31)
+    with Ensemble(slots_per_class=2) as ens:
+        a = ens.submit(256, p, *case, nsteps=3, precision="fp32")
+        ens.run()
+        assert ens.query(a)["state"] == "done"
+        _same(ens.result(a), _solo(256, p, case, 3, "fp32"))
