@@ -9,6 +9,13 @@ summed over replicas).  `e2e` is the same metric through the public API with
 host buffers: the upload of the state from pinned host memory, K steps each
 returning its diagnostics to the host, and the download of the state.
 
+On one GPU the line also carries the north star's two other forms:
+`fp32_refine` (the FP32 + FP64-residual refinement form on the same workload:
+its step time, speed-up over the FP64 form and per-kernel roofline, and its
+errors against the FP64 form of the same discrete problem after the same
+steps) and `serving` (a seeded stream of --serve-requests requests served by
+the ensemble in both forms and one at a time with the plain form).
+
 Multi-GPU: the step does not shard (one simulation per GPU), so N ranks run N
 independent replicas of the workload ("replicas only", weak scaling); there is
 no collective on the data path.
@@ -78,7 +85,9 @@ def kernel_bytes_per_point(n: int, pf: bool, precision: str = "fp64") -> dict:
         # write the half spectrum; the same column passes; write dp.  The
         # projection also reads dp.
         kb.update({"xres": 4 * e + spec, "yfwd2": 2 * spec, "zsolve2": 2 * spec, "yinv2": 2 * spec,
-                   "xinv2": spec + e, "project": 8 * e})
+                   "xinv2": spec + e, "project": 8 * e,
+                   # fused: read the correction spectrum, p0, ustar(3); write u,v,w
+                   "xinvproj": spec + 7 * e})
     return kb
 
 
@@ -106,10 +115,13 @@ def parse(argv=None):
     ap.add_argument("--dt", type=float, default=2e-4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-fp32", action="store_true", help="skip the FP32 refinement form's sub-record")
+    ap.add_argument("--no-serve", action="store_true", help="skip the served-ensemble sub-record")
+    ap.add_argument("--serve-requests", type=int, default=32)
     return ap.parse_args(argv)
 
 
-def workload(n, pf, dt, precision="fp64"):
+def workload_params(n, dt, precision="fp64"):
     from mhit36_b200 import fields
     from mhit36_b200.config import InputParams
     # the FP32 refinement form solves with the FD-modified k^2 (the symbol of
@@ -120,6 +132,12 @@ def workload(n, pf, dt, precision="fp64"):
         recipe = (64, 0.2, 0.35)
     else:
         recipe = fields.DROP_RECIPES.get(n, (8, 0.4, 0.6))
+    return p, None, recipe
+
+
+def workload(n, pf, dt, precision="fp64"):
+    from mhit36_b200 import fields
+    p, _, recipe = workload_params(n, dt, precision)
     u, v, w = fields.random_velocity(n, n)
     phi = None
     if pf:
@@ -284,6 +302,75 @@ def replicas_rate(world: int, npts: int, steps: int, seconds: float) -> float:
     return world * npts * steps / seconds / 1e6
 
 
+def timed_steps(s, steps, warmup):
+    """ms per step of `steps` graph replays on the solver's stream (CUDA events)."""
+    import torch
+    stream = torch.cuda.ExternalStream(s.stream())
+    s.step(warmup)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    s.step_async(steps)
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def fp32_refine_leg(n, pf, case, args, ms64, peak):
+    """The FP32 + FP64-residual refinement form on the same workload: its own
+    step time, per-kernel roofline and speed-up over the FP64 form, then its
+    errors against the FP64 form of the same discrete problem (FD-modified
+    k^2 in both) after the same number of steps."""
+    from mhit36_b200 import Solver
+    p, _, _ = workload_params(n, args.dt, "fp32")
+    npts = n ** 3
+    with Solver(n, p, precision="fp32", phase_field=pf) as s:
+        s.set_fields(*case)
+        ms = timed_steps(s, args.steps, args.warmup)
+        prof = s.profile_step(3)
+        d = s.step(0)  # diagnostics of the last step, max |div u| of its FP64 projection
+        st32 = s.stats()
+        f32 = s.get_fields()
+    total = args.warmup + args.steps + 3
+    with Solver(n, p, precision="fp64", phase_field=pf) as s:
+        s.set_fields(*case)
+        s.step(total)
+        st64 = s.stats()
+        f64 = s.get_fields()
+    rel = lambda a, b: float(np.max(np.abs(a - b)) / np.max(np.abs(b)))  # noqa: E731
+    errs = {name: rel(a, b) for name, a, b in zip(("u", "v", "w", "phi"), f32, f64) if b is not None}
+    kb = kernel_bytes_per_point(n, pf, "fp32")
+    step_bytes = ALGO_BYTES_STEP["fp32"][pf] * npts
+    return {"ms_per_step": ms, "value": npts / (ms / 1e3) / 1e6, "unit": UNIT,
+            "speedup_vs_fp64": ms64 / ms, "dtype": "f32 (FP64 residual, projection, reductions)",
+            "per_kernel_ms": {k: round(v, 4) for k, v in prof.items()},
+            "per_kernel_gbs": {k: round(kb[k] * npts / (v / 1e3) / 1e9, 1) for k, v in prof.items() if kb.get(k)},
+            "step": {"algo_bytes_per_point": ALGO_BYTES_STEP["fp32"][pf],
+                     "achieved": step_bytes / (ms / 1e3) / 1e9, "frac": step_bytes / (ms / 1e3) / 1e9 / peak},
+            "errors_vs_fp64": {"after_steps": total, "max_div_fp64_projection": d["max_div"],
+                               "ke_rel": abs(st32["ke"] / st64["ke"] - 1),
+                               "dissipation_rel": abs(st32["dissipation"] / st64["dissipation"] - 1),
+                               **{f"{k}_rel_to_max": v for k, v in errs.items()}},
+            "k2_mode": "FD-modified (both forms, for the error comparison)", "status": d["status"]}
+
+
+def serving_leg(nreq):
+    """A bounded seeded stream through the served ensemble, both forms,
+    against the same requests one at a time with the plain FP64 form."""
+    from mhit36_b200.serve_bench import run_stream
+    out = {}
+    for line in run_stream(requests=nreq, forms=("fp64", "fp32")):
+        out[line["form"]] = {k: line[k] for k in ("steps_per_s", "p50_latency_s", "p99_latency_s",
+                                                   "vs_sequential_plain", "failed", "bitwise_same_as_alone",
+                                                   "device_only_plain_steps_per_s")}
+        out["sequential_plain"] = line["sequential_plain"]
+        out["requests"] = line["requests"]
+        out["total_steps"] = line["total_steps"]
+        out["sizes"] = line["sizes"]
+    return out
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -384,6 +471,16 @@ def main():
                "d2h_bytes_per_step": nf * npts * 8 / args.steps + 88,
                "ms_per_step": el / args.steps * 1e3}
 
+    mem_bytes = s.memory_bytes()
+    s.close()
+    # the other two forms of the north star, on one GPU only: the FP32
+    # refinement form on the same workload, and a bounded served stream
+    fp32 = serving = None
+    if world == 1 and args.precision == "fp64" and not args.no_fp32:
+        fp32 = fp32_refine_leg(n, pf, case, args, step_ms, peak)
+    if world == 1 and not args.no_serve and args.serve_requests > 0:
+        serving = serving_leg(args.serve_requests)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, st, thr, el = cpu_oracle_rate(n, pf, args.dt, (p, case), max_seconds=20.0)
@@ -401,12 +498,12 @@ def main():
                                    f"{recipe[0] if pf else 0} drops r in [{recipe[1]},{recipe[2]}]",
                        "n": n, "phase_field": pf, "precision": args.precision, "dt": args.dt, "mu": 6e-3,
                        "lin_force": 0.1, "parallelism": f"replicas x{world}",
-                       "l2": "state larger than L2 (resident fields ~{:.0f} GB)".format(s.memory_bytes() / 1e9)},
+                       "l2": "state larger than L2 (resident fields ~{:.0f} GB)".format(mem_bytes / 1e9)},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": clk, "status": diag["status"], "umax": diag["umax"], "cfl": diag["cfl"],
+            "fp32_refine": fp32, "serving": serving,
         }
         print(json.dumps(line), flush=True)
-    s.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

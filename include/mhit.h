@@ -84,7 +84,9 @@ typedef struct mhit_diag {
   double cfl;      /* gumax*dt*dxi (multi/main.f90:942) */
   double umean, vmean, wmean; /* means removed by the step (multi/main.f90:906-919) */
   double gamma;    /* ACDI gamma used by the next step (1.0*gumax, multi/main.f90:362) */
-  double max_div;  /* FP32 refine form: max |div u| of the FP64 projection; -1 in the FP64 form */
+  double max_div;  /* FP32 refine form: max |div u| of the last step's FP64 projection (from 256^3 up
+                      measured when mhit_step / mhit_get_diag return, from the stored ustar, p0 and
+                      correction spectrum); -1 in the FP64 form */
   int64_t step;    /* steps taken since set_fields/load */
   int32_t status;  /* MHIT_OK or the sticky device error */
   int32_t reserved;
@@ -135,7 +137,9 @@ int mhit_get_fields(mhit_handle* h, double* u, double* v, double* w, double* phi
 /* Download the last pressure p (multi/main.f90:842-850).  From 256^3 up the
  * FP64 step fuses the x inverse FFT into the projection and does not store
  * p; this call then recomputes it from the last step's spectrum (one x
- * inverse pass on the device) before the download. */
+ * inverse pass on the device) before the download.  The FP32 refinement form
+ * returns p0 + dp, recomputing dp from the correction solve's spectrum the
+ * same way. */
 int mhit_get_pressure(mhit_handle* h, double* p, int layout);
 
 /*
@@ -311,6 +315,11 @@ int mhit_ens_submit(mhit_ensemble* e, const mhit_params* p, int n, int precision
  * requests, activate uploaded ones, admit what fits, and keep a few
  * milliseconds of batched steps queued on every busy class. */
 int mhit_ens_progress(mhit_ensemble* e, int* pending);
+/* Sleep until a scheduling round has something to do (a transfer finished,
+ * a class has room for more rounds, a request can be retired) or timeout_s
+ * passes; *ready = 1 or 0.  A serving loop alternates mhit_ens_progress and
+ * mhit_ens_wait instead of spinning on mhit_ens_progress. */
+int mhit_ens_wait(mhit_ensemble* e, double timeout_s, int* ready);
 int mhit_ens_query(mhit_ensemble* e, int64_t id, mhit_ens_info* out);
 /* Final fields of a done request (keep_result = 1), raw layout float64. */
 int mhit_ens_result(mhit_ensemble* e, int64_t id, double* u, double* v, double* w, double* phi);

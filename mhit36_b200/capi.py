@@ -88,7 +88,7 @@ HEADER_SYMBOLS = [
     "mhit_device_state", "mhit_sync_state", "mhit_memory_bytes", "mhit_launches_per_step",
     "mhit_destroy", "mhit_strerror", "mhit_size_supported", "mhit_profile_step", "mhit_stage_name",
     "mhit_step_async", "mhit_stream", "mhit_last_error", "mhit_diagnostics", "mhit_poisson_noalloc",
-    "mhit_ens_create", "mhit_ens_submit", "mhit_ens_progress", "mhit_ens_query", "mhit_ens_result",
+    "mhit_ens_create", "mhit_ens_submit", "mhit_ens_progress", "mhit_ens_wait", "mhit_ens_query", "mhit_ens_result",
     "mhit_ens_release", "mhit_ens_cancel", "mhit_ens_stats", "mhit_ens_last_error", "mhit_ens_destroy",
     "mhit_set_tiles", "mhit_drop_count",
 ]
@@ -139,6 +139,7 @@ def load_library(path: str = LIB_PATH):
         "mhit_ens_submit": (ctypes.c_int, [H, P(MhitParams), ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                            dp, dp, dp, dp, ctypes.c_int, P(ctypes.c_int64)]),
         "mhit_ens_progress": (ctypes.c_int, [H, P(ctypes.c_int)]),
+        "mhit_ens_wait": (ctypes.c_int, [H, ctypes.c_double, P(ctypes.c_int)]),
         "mhit_ens_query": (ctypes.c_int, [H, ctypes.c_int64, P(MhitEnsInfo)]),
         "mhit_ens_result": (ctypes.c_int, [H, ctypes.c_int64, dp, dp, dp, dp]),
         "mhit_ens_release": (ctypes.c_int, [H, ctypes.c_int64]),

@@ -36,6 +36,7 @@
 #include <chrono>
 #include <condition_variable>
 #include <deque>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -142,10 +143,14 @@ class Transfer {
     if ((e = cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking))) return e;
     for (int k = 0; k < 2; ++k) {
       if ((e = cudaMallocHost(&stage_[k], kChunk))) return e;
-      if ((e = cudaEventCreateWithFlags(&sev_[k], cudaEventDisableTiming))) return e;
+      // blocking-sync events: a transfer thread waiting for a copy sleeps
+      // instead of spinning on a core the other transfer threads and the
+      // scheduling thread need
+      if ((e = cudaEventCreateWithFlags(&sev_[k], cudaEventDisableTiming | cudaEventBlockingSync))) return e;
       if ((e = cudaEventRecord(sev_[k], st_))) return e;
     }
     if ((e = cudaMallocHost(&small_, kSmall))) return e;
+    if ((e = cudaEventCreateWithFlags(&jev_, cudaEventDisableTiming | cudaEventBlockingSync))) return e;
     th_ = std::thread([this] { loop(); });
     return cudaSuccess;
   }
@@ -170,8 +175,10 @@ class Transfer {
     }
     for (int k = 0; k < 2; ++k) {
       if (sev_[k]) cudaEventDestroy(sev_[k]);
+      if (k == 0 && jev_) cudaEventDestroy(jev_);
       if (stage_[k]) cudaFreeHost(stage_[k]);
       sev_[k] = nullptr;
+      if (k == 0) jev_ = nullptr;
       stage_[k] = nullptr;
     }
     if (small_) cudaFreeHost(small_);
@@ -199,8 +206,21 @@ class Transfer {
         cudaGetLastError();
       }
       (j.kind == 0 ? j.r->up : j.r->down).store(e == cudaSuccess ? IO_DONE : IO_FAILED);
+      if (notify_) notify_();
     }
   }
+
+ public:
+  // called after every finished job (wakes mhit_ens_wait)
+  std::function<void()> notify_;
+
+  // wait for every copy issued on the transfer stream so far (sleeping)
+  cudaError_t sync() {
+    cudaError_t e = cudaEventRecord(jev_, st_);
+    return e ? e : cudaEventSynchronize(jev_);
+  }
+
+ private:
 
   // host float64 -> device field of `el` bytes per value, chunk by chunk
   cudaError_t put(void* dst, const double* src, size_t count, size_t el) {
@@ -268,6 +288,7 @@ class Transfer {
   cudaStream_t st_ = nullptr;
   void* stage_[2] = {nullptr, nullptr};
   cudaEvent_t sev_[2] = {nullptr, nullptr};
+  cudaEvent_t jev_ = nullptr;  // end of a job's copies (blocking sync)
   void* small_ = nullptr;
   int k_ = 0;
   std::thread th_;
@@ -298,6 +319,11 @@ struct mhit_ensemble {
   bool xfer_started = false;
   std::string last_error;
   long long rounds = 0, launches = 0;
+  // mhit_ens_wait sleeps on this until a transfer thread finishes a job (or
+  // a short interval passes, after which it looks at the class streams)
+  std::mutex wait_mu;
+  std::condition_variable wait_cv;
+  unsigned long long io_done = 0;
 };
 
 namespace {
@@ -669,7 +695,7 @@ cudaError_t Transfer::upload(const Job& j, std::string* where) {
   ctl->beta = 0.0;
   ctl->cfl_limit = r->prm.cfl_limit > 0 ? r->prm.cfl_limit : 7.0;
   TCK(cudaMemcpyAsync(b.ctrl, ctl, sizeof(Ctrl), cudaMemcpyHostToDevice, st_));
-  TCK(cudaStreamSynchronize(st_));  // the small area and the caller's input are free again
+  TCK(sync());  // the small area and the caller's input are free again
   return cudaSuccess;
 }
 
@@ -683,7 +709,7 @@ cudaError_t Transfer::download(const Job& j, std::string* where) {
   cudaError_t e;
   Ctrl* ctl = reinterpret_cast<Ctrl*>(small_);
   TCK(cudaMemcpyAsync(ctl, b.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st_));
-  TCK(cudaStreamSynchronize(st_));
+  TCK(sync());
   r->fin = *ctl;
   if (r->keep) {
     const void* src[4] = {b.f[0], b.f[1], b.f[2], b.f[13]};
@@ -843,6 +869,33 @@ void wait_io(const std::atomic<int>& s) {
   for (int it = 0; s.load() == IO_QUEUED && it < 1200000; ++it) std::this_thread::sleep_for(std::chrono::microseconds(100));
 }
 
+// Whether a scheduling round now has something to do: a transfer job of a
+// request finished, a retiring request's class stream passed its retirement,
+// an autotuner trial finished (or can start), or a busy class has room in its
+// queue of rounds.
+bool work_ready(mhit_ensemble* e) {
+  for (auto& kv : e->reqs) {
+    Request* r = kv.second.get();
+    if (r->loading && r->up.load() != IO_QUEUED) return true;
+    if (r->finishing) {
+      const int d = r->down.load();
+      if (d == IO_DONE || d == IO_FAILED) return true;
+      if (d == IO_NONE && cudaEventQuery(r->done_ev) != cudaErrorNotReady) return true;
+    }
+  }
+  for (auto& cp : e->classes) {
+    Class* c = cp.get();
+    if (!c->tuned) {
+      if (c->trial_pending ? cudaEventQuery(c->ev1) != cudaErrorNotReady : !c->running.empty()) return true;
+      continue;
+    }
+    if (c->running.empty()) continue;
+    if ((int)c->inflight.size() < queue_depth(c)) return true;
+    if (cudaEventQuery(c->inflight.front()) != cudaErrorNotReady) return true;
+  }
+  return false;
+}
+
 }  // namespace
 
 extern "C" {
@@ -857,6 +910,15 @@ int mhit_ens_create(size_t hbm_budget_bytes, int slots_per_class, mhit_ensemble*
   e->budget = hbm_budget_bytes ? hbm_budget_bytes : (size_t)(0.85 * (double)freeb);
   e->slots_per_class = slots_per_class;
   e->t0 = now_s();
+  mhit_ensemble* ep = e.get();
+  for (auto& x : e->xfer)
+    x.notify_ = [ep] {
+      {
+        std::lock_guard<std::mutex> g(ep->wait_mu);
+        ++ep->io_done;
+      }
+      ep->wait_cv.notify_all();
+    };
   bool ok = true;
   for (auto& x : e->xfer) ok = ok && x.start(e->device) == cudaSuccess;
   if (!ok) {
@@ -1045,6 +1107,38 @@ int mhit_ens_progress(mhit_ensemble* e, int* pending) {
   for (auto& kv : e->reqs)
     if (kv.second->state == RQ_QUEUED || kv.second->state == RQ_RUNNING) ++pend;
   if (pending) *pending = pend;
+  if (dev >= 0 && dev != e->device) cudaSetDevice(dev);
+  return MHIT_OK;
+}
+
+// Sleep until a scheduling round has something to do, or `timeout_s`
+// passes: *ready = 1 or 0.  Transfer threads wake it when a job finishes;
+// the class streams are looked at every 200 us (their queues hold a few
+// milliseconds of rounds, so nothing idles meanwhile).
+int mhit_ens_wait(mhit_ensemble* e, double timeout_s, int* ready) {
+  if (!e || !(timeout_s >= 0)) return MHIT_ERR_INVALID;
+  int dev = -1;
+  cudaGetDevice(&dev);
+  if (dev != e->device) cudaSetDevice(e->device);
+  const double deadline = now_s() + timeout_s;
+  int rdy = 0;
+  for (;;) {
+    unsigned long long seen;
+    {
+      std::lock_guard<std::mutex> g(e->wait_mu);
+      seen = e->io_done;
+    }
+    if (work_ready(e)) {
+      rdy = 1;
+      break;
+    }
+    const double left = deadline - now_s();
+    if (left <= 0) break;
+    std::unique_lock<std::mutex> g(e->wait_mu);
+    e->wait_cv.wait_for(g, std::chrono::microseconds((long long)std::min(left * 1e6, 200.0) + 1),
+                        [&] { return e->io_done != seen; });
+  }
+  if (ready) *ready = rdy;
   if (dev >= 0 && dev != e->device) cudaSetDevice(dev);
   return MHIT_OK;
 }

@@ -3,8 +3,9 @@
 Requests of uneven grid sizes are queued, admitted as slots and HBM free up,
 kept resident and advanced together by per-class CUDA graphs of batched
 kernels (one graph per grid size / precision / phase-field class).  The
-driver calls ``progress()`` in a loop; each call admits what fits and
-advances every busy class by one step.
+driver calls ``progress()`` in a loop, with ``wait()`` between calls; each
+progress call admits what fits and keeps a few milliseconds of batched steps
+queued on every busy class.
 """
 from __future__ import annotations
 
@@ -75,6 +76,12 @@ class Ensemble:
         self._check(self.lib.mhit_ens_progress(self.h, ctypes.byref(pending)), "mhit_ens_progress")
         return pending.value
 
+    def wait(self, timeout: float) -> bool:
+        """Sleep until progress() has something to do (True) or `timeout` s pass (False)."""
+        ready = ctypes.c_int()
+        self._check(self.lib.mhit_ens_wait(self.h, float(timeout), ctypes.byref(ready)), "mhit_ens_wait")
+        return bool(ready.value)
+
     def query(self, rid: int) -> dict:
         info = MhitEnsInfo()
         self._check(self.lib.mhit_ens_query(self.h, rid, ctypes.byref(info)), "mhit_ens_query")
@@ -105,8 +112,10 @@ class Ensemble:
         return {k: getattr(st, k) for k, _ in st._fields_}
 
     def run(self, max_rounds: int = 10 ** 9) -> None:
-        """Progress until nothing is queued or running."""
+        """Progress until nothing is queued or running, sleeping between
+        rounds until there is something to do."""
         for _ in range(max_rounds):
             if self.progress() == 0:
                 return
+            self.wait(0.01)
         raise RuntimeError("ensemble did not drain")

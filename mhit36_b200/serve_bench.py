@@ -114,10 +114,13 @@ def serve(reqs, arrivals, precision, slots):
                                          precision=precision, keep=True, borrow=True)
                 nxt += 1
             pending = ens.progress()
+            to_next = arrivals[order[nxt]] - (time.perf_counter() - t0) if nxt < len(order) else None
             if pending == 0:
                 if nxt >= len(order):
                     break
-                time.sleep(max(0.0, arrivals[order[nxt]] - (time.perf_counter() - t0)))
+                time.sleep(max(0.0, to_next))
+            else:  # sleep until the ensemble has work for a round, or the next arrival
+                ens.wait(0.01 if to_next is None else max(0.0, min(0.01, to_next)))
         lat, done, subm, fails, same = [], [], [], 0, []
         for r in reqs:
             q = ens.query(ids[r["i"]])
@@ -136,17 +139,11 @@ def serve(reqs, arrivals, precision, slots):
     return np.array(done), np.array(lat), fails, same, st, first
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--requests", type=int, default=256)
-    ap.add_argument("--forms", default="fp64,fp32")
-    ap.add_argument("--sizes", default="64,96,128,192,256")
-    ap.add_argument("--slots", type=int, default=8)
-    ap.add_argument("--load", type=float, default=4.0)
-    ap.add_argument("--seed", type=int, default=2024)
-    a = ap.parse_args()
-    sizes = [int(x) for x in a.sizes.split(",")]
-    reqs, gaps = make_stream(a.requests, a.seed, sizes)
+def run_stream(requests=256, forms=("fp64", "fp32"), sizes=(64, 96, 128, 192, 256), slots=8, load=4.0,
+               seed=2024, log=None):
+    """Serve one seeded stream one request at a time (plain FP64) and through
+    the ensemble in each form; returns one result dict per form."""
+    reqs, gaps = make_stream(requests, seed, list(sizes))
     t = time.perf_counter()
     build_inputs(reqs)
     gen_s = time.perf_counter() - t
@@ -164,11 +161,11 @@ def main():
                 t = time.perf_counter()
                 s.step(20)  # returns after the device finished (diagnostics read back)
                 step_s[(n, pf)] = (time.perf_counter() - t) / 20
-    with Ensemble(slots_per_class=a.slots) as ens:
+    with Ensemble(slots_per_class=slots) as ens:
         for n in sizes:
             case = [raw(x) for x in fields.random_velocity(n, 1)]
             phi = raw(fields.drop_field(n, *fields.place_drops(n, 1, 2, 0.3, 0.5)))
-            for form in a.forms.split(","):
+            for form in forms:
                 for pf in (False, True):
                     ens.submit(n, params(reqs[0], form), *case, phi if pf else None, nsteps=2, precision=form)
         ens.run()
@@ -177,27 +174,44 @@ def main():
     # what the stream costs the device alone, one request after another: the
     # bound a server reaches by hiding all host work without batching gains
     device_s = sum(r["steps"] * step_s[(r["n"], r["pf"])] for r in reqs)
-    rate = a.load * len(reqs) / service.sum()  # requests per second offered
+    rate = load * len(reqs) / service.sum()  # requests per second offered
     arrivals = np.cumsum(gaps) / rate
     arrivals -= arrivals[0]
     sdone, slat = replay_fifo(arrivals, service)
     seq = {"steps_per_s": total_steps / (sdone.max() - arrivals.min()),
            "busy_steps_per_s": total_steps / service.sum(),
            "p50_s": float(np.percentile(slat, 50)), "p99_s": float(np.percentile(slat, 99))}
-    for form in a.forms.split(","):
-        done, lat, fails, same, st, first = serve(reqs, arrivals, form, a.slots)
+    out = []
+    for form in forms:
+        done, lat, fails, same, st, first = serve(reqs, arrivals, form, slots)
         agg = total_steps / (np.max(done) - first)
         line = {"metric": "served ensemble: aggregate steps/s and request latency", "form": form,
-                "requests": len(reqs), "total_steps": total_steps, "offered_load_vs_sequential": a.load,
+                "requests": len(reqs), "total_steps": total_steps, "offered_load_vs_sequential": load,
                 "steps_per_s": agg, "p50_latency_s": float(np.percentile(lat, 50)),
                 "p99_latency_s": float(np.percentile(lat, 99)), "failed": fails,
                 "vs_sequential_plain": agg / seq["steps_per_s"], "sequential_plain": seq,
                 "bitwise_same_as_alone": (sum(same), len(same)) if same else None,
-                "ensemble": {"slots_per_class": a.slots, "classes": st["classes"], "rounds": st["rounds"],
+                "ensemble": {"slots_per_class": slots, "classes": st["classes"], "rounds": st["rounds"],
                              "graph_launches": st["graph_launches"]},
-                "sizes": sizes, "input_generation_s": gen_s,
+                "sizes": list(sizes), "input_generation_s": gen_s,
                 "device_only_plain_steps_per_s": total_steps / device_s}
-        print(json.dumps(line), flush=True)
+        if log:
+            log(line)
+        out.append(line)
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--requests", type=int, default=256)
+    ap.add_argument("--forms", default="fp64,fp32")
+    ap.add_argument("--sizes", default="64,96,128,192,256")
+    ap.add_argument("--slots", type=int, default=8)
+    ap.add_argument("--load", type=float, default=4.0)
+    ap.add_argument("--seed", type=int, default=2024)
+    a = ap.parse_args()
+    run_stream(a.requests, a.forms.split(","), [int(x) for x in a.sizes.split(",")], a.slots, a.load, a.seed,
+               log=lambda line: print(json.dumps(line), flush=True))
 
 
 if __name__ == "__main__":
