@@ -313,8 +313,9 @@ template <int N, class T> struct RCfg {
   static constexpr bool ON = (N & (N - 1)) == 0;
   // Register caps per thread (via the resident CTAs per SM the kernels are
   // built for): FP64 y passes 80 (3 CTAs of 256 threads), FP64 z solve 128
-  // (a cap of 80 spilled and measured 24% slower), FP32 y passes 64, FP32 z
-  // solve 40 (measured on B200 at 512^3: 0.68 -> 0.57 ms against no cap).
+  // (a cap of 80 spilled and measured 24% slower), FP32 passes 40, 3 CTAs of
+  // 512 threads (measured on B200 at 512^3: z solve 0.68 -> 0.57 ms against no
+  // cap, y passes 0.245 -> 0.234 ms against 64).
   // FP64: the next slab is prefetched into shared memory with cp.async while
   // the current one is transformed (512^3: y passes 0.48 -> 0.41 ms, z solve
   // 0.94 -> 0.88 ms); the FP32 passes are faster without (0.24 vs 0.25 and
@@ -324,7 +325,7 @@ template <int N, class T> struct RCfg {
   static constexpr bool PF = sizeof(T) == 8;
   static constexpr bool stw(int) { return true; }
   static constexpr int minb(int kind) {
-    const int r = sizeof(T) == 8 ? (kind == 2 ? 128 : 80) : (kind == 2 ? 40 : 64);
+    const int r = sizeof(T) == 8 ? (kind == 2 ? 128 : 80) : 40;
     return 65536 / (NT * r) > 1 ? 65536 / (NT * r) : 1;
   }
 };
