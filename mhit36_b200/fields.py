@@ -61,23 +61,10 @@ def taylor_green(n: int, grid_mode: int = 0):
     return u, v, w
 
 
-def random_velocity(n: int, seed: int, rms: float = 1.0, kp: float = 4.0):
-    """Random-phase solenoidal velocity with E(k) ~ k^4 exp(-2 (k/kp)^2).
-
-    Built in index space (period n cells) on the band |k_i| <= kmax =
-    min(n/2 - 1, 8 kp) (E(8 kp) / E(kp) ~ 1e-53, so nothing is lost): uniform
-    random phases from seeded numpy PCG64, shell amplitude
-    sqrt(E(k) / (4 pi k^2)), projection onto k-perpendicular, the u/v/w
-    components sampled at their staggered faces (half a cell back along
-    x/y/z), then the mean removed and one common factor applied so that the
-    per-component rms averages to `rms` (a common factor keeps the field
-    solenoidal).
-    """
-    try:
-        from scipy import fft as sfft
-        irfftn = lambda G: sfft.irfftn(G, s=(n, n, n), axes=(0, 1, 2), workers=-1)  # noqa: E731
-    except ImportError:  # pragma: no cover
-        irfftn = lambda G: np.fft.irfftn(G, s=(n, n, n), axes=(0, 1, 2))  # noqa: E731
+def velocity_band(n: int, seed: int, kp: float = 4.0):
+    """The seeded spectral band of random_velocity: (ix, iz, F) with F[c] the
+    complex amplitudes of component c on the half-spectrum index grid
+    np.ix_(ix, ix, iz) of an (n, n, n//2+1) array (axes x, y, z)."""
     rng = np.random.Generator(np.random.PCG64(seed))
     kmax = min(n // 2 - 1, int(round(8 * kp)))
     kk = np.arange(-kmax, kmax + 1, dtype=np.float64)
@@ -105,6 +92,27 @@ def random_velocity(n: int, seed: int, rms: float = 1.0, kp: float = 4.0):
     F[2] *= np.exp(-1j * np.pi * KZ / n)
     ix = (np.arange(-kmax, kmax + 1) % n)
     iz = np.arange(0, kmax + 1)
+    return ix, iz, F
+
+
+def random_velocity(n: int, seed: int, rms: float = 1.0, kp: float = 4.0):
+    """Random-phase solenoidal velocity with E(k) ~ k^4 exp(-2 (k/kp)^2).
+
+    Built in index space (period n cells) on the band |k_i| <= kmax =
+    min(n/2 - 1, 8 kp) (E(8 kp) / E(kp) ~ 1e-53, so nothing is lost): uniform
+    random phases from seeded numpy PCG64, shell amplitude
+    sqrt(E(k) / (4 pi k^2)), projection onto k-perpendicular, the u/v/w
+    components sampled at their staggered faces (half a cell back along
+    x/y/z), then the mean removed and one common factor applied so that the
+    per-component rms averages to `rms` (a common factor keeps the field
+    solenoidal).
+    """
+    try:
+        from scipy import fft as sfft
+        irfftn = lambda G: sfft.irfftn(G, s=(n, n, n), axes=(0, 1, 2), workers=-1)  # noqa: E731
+    except ImportError:  # pragma: no cover
+        irfftn = lambda G: np.fft.irfftn(G, s=(n, n, n), axes=(0, 1, 2))  # noqa: E731
+    ix, iz, F = velocity_band(n, seed, kp)
     out = []
     for c in range(3):
         G = np.zeros((n, n, n // 2 + 1), dtype=np.complex128)
