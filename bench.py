@@ -54,13 +54,14 @@ UNIT = "Mpts*steps/s"
 # second solve.
 ALGO_BYTES_STEP = {"fp64": {True: 280, False: 232}, "fp32": {True: 200, False: 176}}
 
-# DRAM bytes (read + write) per grid point per launch, from one ncu capture of
+# DRAM bytes (read + write) per grid point per launch, from ncu captures of
 # the FP64 kernels at 256^3 (dram__bytes_read.sum + dram__bytes_write.sum of
-# each launch / 256^3; the summary is profiles/kernels_fp64_256_full.md).  A
-# stencil or column pass touches every point the same way at any size, so
-# traffic scales with the points processed; a full 512^3 capture is too large
-# to take under ncu.
-DRAM_BYTES_PER_POINT_FP64 = {"momentum": 103.91, "phase": 40.55, "project": 54.13, "xfwd": 30.80,
+# a launch / 256^3; summaries in profiles/momentum_fp64_256_full.md,
+# profiles/phase_fp64_256_full.md and, for the Poisson kernels,
+# profiles/kernels_fp64_256_full.md).  A stencil or column pass touches every
+# point the same way at any size, so traffic scales with the points
+# processed; a full 512^3 capture is too large to take under ncu.
+DRAM_BYTES_PER_POINT_FP64 = {"momentum": 103.86, "phase": 40.18, "project": 54.13, "xfwd": 30.80,
                              "yfwd": 13.59, "zsolve": 13.64, "yinv": 13.59, "xinv": 13.82, "xinvproj": 55.30}
 
 
