@@ -1,17 +1,9 @@
-// Shared-memory batched FFT for libmhit.
+// FFT building blocks of libmhit: radix-2/3/4/8 butterflies and the
+// register-resident line transform (reg_fft_stages) that every x, y and z
+// pass of the Poisson solve uses.
 //
-// A CTA holds L complex lines of length N in shared memory, interleaved so
-// that element n of line l sits at s[n*LP + l] with the row pitch LP = L + 1
-// ("column-major": the L lines are the fast axis; the one-element pad per row
-// keeps both the stage accesses and x-fastest staging writes free of bank
-// conflicts).  That is the layout of a chunk of L consecutive kx
-// columns of the spectrum, so the y and z passes stage 128-byte rows straight
-// from HBM, and every Stockham stage below reads and writes 32 consecutive
-// elements per warp (no shared-memory bank conflicts for 8- or 16-byte
-// elements).
-//
-// The transform is the Stockham autosort formulation (natural-order output,
-// in place through registers): for each stage with radix R and span Ns,
+// The transform is the Stockham autosort formulation (natural-order output):
+// for each stage with radix R and span Ns,
 //   v[r] = x[j + r*N/R] * w_N^(DIR * r*(j mod Ns)*N/(Ns*R)),  v = DFT_R(v),
 //   x'[(j/Ns)*Ns*R + (j mod Ns) + r*Ns] = v[r].
 // DIR = -1 is the forward transform e^{-2 pi i jk/N} (cuFFT's
@@ -22,10 +14,6 @@
 #include "common.cuh"
 
 namespace mhit {
-
-constexpr int pick_radix(int rem) {
-  return rem % 8 == 0 ? 8 : (rem % 4 == 0 ? 4 : (rem % 2 == 0 ? 2 : (rem % 3 == 0 ? 3 : rem)));
-}
 
 template <int R, int DIR, class C> struct DFT;
 
@@ -91,88 +79,22 @@ template <int DIR, class C> struct DFT<3, DIR, C> {
   }
 };
 
-// One Stockham stage over L interleaved lines, NT threads.
-template <int L> struct Pitch { static constexpr int value = L + 1; };
-
-// Identity post-processing of a stage's outputs.
-struct NoPost {
-  template <class C> __device__ __forceinline__ C operator()(int, int, C v) const { return v; }
-};
-
-// `post(k, l, v)` is applied to every output of the stage (k: index along the
-// line, l: line) before it is stored; the last stage of a transform uses it
-// to fuse a per-mode scaling.
-template <int N, int R, int NS, int L, int NT, int DIR, class C, class Post = NoPost>
-__device__ __forceinline__ void fft_stage(C* s, const C* __restrict__ tw, const Post& post = Post()) {
-  constexpr int LP = Pitch<L>::value;
-  constexpr int NR = N / R;
-  constexpr int W = L * NR;
-  constexpr int ITEMS = (W + NT - 1) / NT;
-  constexpr int TSTRIDE = N / (NS * R);
-  C v[ITEMS][R];
-#pragma unroll
-  for (int it = 0; it < ITEMS; ++it) {
-    const int wi = threadIdx.x + it * NT;
-    if ((ITEMS * NT == W) || wi < W) {
-      const int l = wi % L, j = wi / L;
-      const int jm = j % NS;
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        C a = s[(j + r * NR) * LP + l];
-        if (NS > 1 && r > 0) {
-          C t = tw[r * jm * TSTRIDE];
-          a = (DIR < 0) ? cmul(a, t) : cmulc(a, t);
-        }
-        v[it][r] = a;
-      }
-      DFT<R, DIR, C>::run(v[it]);
-    }
-  }
-  __syncthreads();
-#pragma unroll
-  for (int it = 0; it < ITEMS; ++it) {
-    const int wi = threadIdx.x + it * NT;
-    if ((ITEMS * NT == W) || wi < W) {
-      const int l = wi % L, j = wi / L;
-      const int jm = j % NS;
-      const int d0 = (j / NS) * NS * R + jm;
-#pragma unroll
-      for (int r = 0; r < R; ++r) s[(d0 + r * NS) * LP + l] = post(d0 + r * NS, l, v[it][r]);
-    }
-  }
-  __syncthreads();
-}
-
-template <int N, int NS, int L, int NT, int DIR, class C> struct FFTRun {
-  template <class Post>
-  static __device__ __forceinline__ void run(C* s, const C* __restrict__ tw, const Post& post) {
-    if constexpr (NS < N) {
-      constexpr int R = pick_radix(N / NS);
-      if constexpr (NS * R == N) {
-        fft_stage<N, R, NS, L, NT, DIR, C, Post>(s, tw, post);
-      } else {
-        fft_stage<N, R, NS, L, NT, DIR, C>(s, tw);
-        FFTRun<N, NS * R, L, NT, DIR, C>::run(s, tw, post);
-      }
-    }
-  }
-};
-
 // ---------------------------------------------------------------- register-resident lines
-// Power-of-two N: a line is spread over TPC = N/8 threads, each holding eight
-// of its elements in registers, v[m] = x[t + TPC*m] for thread t of the line.
-// Every stage's butterflies run on registers -- butterfly b of the thread is
-// j = t + TPC*b with inputs v[b + (8/R)*r], which are x[j + r*N/R], the
+// A line is spread over TPC = N/E threads, each holding E of its elements in
+// registers, v[m] = x[t + TPC*m] for thread t of the line: E = 8 for
+// power-of-two N, E = 12 for N = 3*2^k (96, 192, 384, 768).  Every stage's
+// radix R divides E (8, 4 or 2 for E = 8; 4, 2, 3 for E = 12, in that
+// order), and its butterflies run on registers -- butterfly b of the thread
+// is j = t + TPC*b with inputs v[b + (E/R)*r], which are x[j + r*N/R], the
 // Stockham map of fft_stage -- and the data crosses shared memory only
 // between stages: a stage writes its outputs at their Stockham positions and
 // the next stage reads the canonical v[m] back.  The last stage's outputs are
 // the canonical positions themselves (NS*R = N makes them x[j + r*N/R]), so
-// they stay in registers.  Each element sees fft_stage's arithmetic in the
-// same order, so both transforms give the same bits.
+// they stay in registers.
 //
 // Exchange buffer: `at(n)` is the shared-memory slot of element n of the
 // thread's line.  The exchanges write either consecutive elements or
-// elements 8 apart (d = 8j + r over consecutive j), and both must be free of
+// elements R apart (d = Rj + r over consecutive j), and both must be free of
 // bank conflicts for the phase a warp's access is split into (8 lanes for
 // 16-byte elements, 16 for 8-byte ones).  Two index maps do that:
 //   * reg_pad: one pad element after every 8 (n + n/8).  Lines are
@@ -187,13 +109,21 @@ template <int N, int NS, int L, int NT, int DIR, class C> struct FFTRun {
 __host__ __device__ constexpr int reg_rows(int N) { return N + N / 8; }
 __device__ __forceinline__ int reg_pad(int n) { return n + (n >> 3); }
 __device__ __forceinline__ int reg_swz(int n) { return n ^ ((n >> 3) & 15); }
+// Elements per thread of a register-resident line of length N.
+__host__ __device__ constexpr int reg_elems(int N) { return (N & (N - 1)) == 0 ? 8 : 12; }
+constexpr int pick_radix_reg(int rem, int E) {
+  return (rem % 8 == 0 && E % 8 == 0) ? 8
+         : (rem % 4 == 0 && E % 4 == 0) ? 4
+         : (rem % 2 == 0 && E % 2 == 0) ? 2
+         : (rem % 3 == 0 && E % 3 == 0) ? 3 : rem;
+}
 
-template <int N, int NS, int DIR, class C, class At>
-__device__ __forceinline__ void reg_fft_stages(C (&v)[8], C* s, const C* __restrict__ tw, int t, const At& at) {
+template <int N, int NS, int DIR, class C, int E, class At>
+__device__ __forceinline__ void reg_fft_stages(C (&v)[E], C* s, const C* __restrict__ tw, int t, const At& at) {
   if constexpr (NS < N) {
-    constexpr int R = pick_radix(N / NS);
-    static_assert(8 % R == 0, "register-resident lines need a power-of-two length");
-    constexpr int B = 8 / R, TPC = N / 8, TSTRIDE = N / (NS * R);
+    constexpr int R = pick_radix_reg(N / NS, E);
+    static_assert(E % R == 0 && (N / NS) % R == 0, "register-resident lines: the radix must divide E");
+    constexpr int B = E / R, TPC = N / E, TSTRIDE = N / (NS * R);
 #pragma unroll
     for (int b = 0; b < B; ++b) {
       const int j = t + TPC * b;
@@ -224,25 +154,11 @@ __device__ __forceinline__ void reg_fft_stages(C (&v)[8], C* s, const C* __restr
       }
       __syncthreads();
 #pragma unroll
-      for (int m = 0; m < 8; ++m) v[m] = s[at(t + TPC * m)];
+      for (int m = 0; m < E; ++m) v[m] = s[at(t + TPC * m)];
       __syncthreads();
-      reg_fft_stages<N, NS * R, DIR, C>(v, s, tw, t, at);
+      reg_fft_stages<N, NS * R, DIR, C, E>(v, s, tw, t, at);
     }
   }
-}
-
-// In-place transform of L interleaved lines of length N held in s.
-// Must be called by all NT threads of the CTA; ends with a barrier.
-template <int N, int L, int NT, int DIR, class C>
-__device__ __forceinline__ void smem_fft(C* s, const C* __restrict__ tw) {
-  FFTRun<N, 1, L, NT, DIR, C>::run(s, tw, NoPost());
-}
-
-// The same, with post(k, l, v) applied to every output (mode k of line l)
-// as the last stage stores it.
-template <int N, int L, int NT, int DIR, class C, class Post>
-__device__ __forceinline__ void smem_fft_post(C* s, const C* __restrict__ tw, const Post& post) {
-  FFTRun<N, 1, L, NT, DIR, C>::run(s, tw, post);
 }
 
 }  // namespace mhit

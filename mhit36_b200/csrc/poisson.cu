@@ -9,10 +9,11 @@
 //     The reference transforms the full complex field (2x the work).
 //   * Spectrum layout in HBM: spec[kz][ky][kx], kx fastest, row pitch PITCH
 //     complex (N/2+1 rounded up to the column chunk CC), so a chunk of CC
-//     kx columns is one 32-128-byte row segment.  The y and z passes stage a
-//     CC x N slab in shared memory, transform along the slow axis there, and
-//     write it back in place: no transposes in HBM at all (the reference does
-//     four cuDecomp transposes per solve, multi/main.f90:754-810).
+//     kx columns is one 32-128-byte row segment.  The y and z passes hold a
+//     CC x N slab of columns in registers (register-resident lines, fft.cuh),
+//     transform along the slow axis and write it back in place: no
+//     transposes in HBM at all (the reference does four cuDecomp transposes
+//     per solve, multi/main.f90:754-810).
 //   * The z pass fuses forward FFT, the k^2 division and the inverse FFT.
 //   * The inverse x pass is complex-to-real for two lines at once.
 #include <cuda_runtime.h>
@@ -33,7 +34,6 @@ template <int N, class T = double> struct PCfg {
   static constexpr int L = (N <= 256) ? 8 : ((N <= 512) ? 4 : 2);
   static constexpr int P = L;                               // line pairs per CTA (x passes)
   static constexpr int CC = (sizeof(T) == 8) ? L : 2 * L;   // kx columns per CTA (y/z passes)
-  static constexpr int NT = 256;
   static constexpr int PITCH = ((N / 2 + 1) + CC - 1) / CC * CC;
   static constexpr int NCHUNK = PITCH / CC;
 };
@@ -68,63 +68,9 @@ __device__ __forceinline__ double xfwd_rhs(const T* __restrict__ us, const T* __
   return r;
 }
 
-template <int N, int MODE, class T>
-__device__ __forceinline__ void xfwd_body(const T* __restrict__ us, const T* __restrict__ vs,
-                                          const T* __restrict__ ws, const T* __restrict__ rhs,
-                                          const T* __restrict__ p0, typename C2<T>::t* __restrict__ spec,
-                                          const typename C2<T>::t* __restrict__ tw, const Ctrl* __restrict__ ctrl,
-                                          double cdiv, double ddxi, int bx, int by) {
-  typedef typename C2<T>::t C;
-  typedef PCfg<N, T> G;
-  constexpr int P = G::P, NT = G::NT;
-  if (ctrl && ctrl->status) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* s = reinterpret_cast<C*>(smem_raw);
-  constexpr int LP = Pitch<P>::value;
-  const int j0 = bx * (2 * P);
-  const int k = by;
-  // x-fastest: each warp reads 32 consecutive cells of the same lines; a
-  // fixed trip count (P*N is a multiple of NT) unrolled by 2 keeps two
-  // elements' loads in flight per thread (measured 15% faster at 512^3; the
-  // residual mode, with the Laplacian's 7 extra loads, is faster without)
-  static_assert((P * N) % NT == 0, "x pass staging assumes whole rounds");
-  constexpr int XU = (MODE == 2) ? 1 : 2;
-#pragma unroll XU
-  for (int it = 0; it < P * N / NT; ++it) {
-    const int wi = threadIdx.x + it * NT;
-    const int n = wi % N, p = wi / N;
-    const int ja = j0 + 2 * p;
-    C z;
-    z.x = (T)xfwd_rhs<N, MODE, T>(us, vs, ws, rhs, p0, cdiv, ddxi, n, ja, k);
-    z.y = (T)xfwd_rhs<N, MODE, T>(us, vs, ws, rhs, p0, cdiv, ddxi, n, ja + 1, k);
-    s[n * LP + p] = z;
-  }
-  __syncthreads();
-  smem_fft<N, P, NT, -1>(s, tw);
-  const T half = (T)0.5;
-  constexpr int M = N / 2 + 1;
-  for (int wi = threadIdx.x; wi < P * M; wi += NT) {
-    const int m = wi % M, p = wi / M;
-    const int ja = j0 + 2 * p;
-    const C zm = s[m * LP + p];
-    const C zr = s[((m == 0) ? 0 : (N - m)) * LP + p];
-    C A, B;
-    A.x = half * (zm.x + zr.x);
-    A.y = half * (zm.y - zr.y);
-    B.x = half * (zm.y + zr.y);
-    B.y = -half * (zm.x - zr.x);
-    C* row = spec + ((size_t)k * N + ja) * G::PITCH;
-    row[m] = A;
-    row[G::PITCH + m] = B;
-  }
-}
-
-// ---------------------------------------------------------------- persistent column passes
-// The y passes and the z solve as persistent kernels: each CTA walks a
-// strided list of (column chunk, line) slabs.  The slab after the current one
-// is copied into the second shared-memory buffer with cp.async while the
-// current one is transformed, so HBM traffic overlaps the FFT arithmetic.
-// KIND 0/1: y pass forward/inverse; KIND 2: z solve.
+// ---------------------------------------------------------------- column slabs
+// The y passes and the z solve walk (column chunk, line) slabs of the half
+// spectrum.  KIND 0/1: y pass forward/inverse; KIND 2: z solve.
 struct ColSlab {
   void* spec;        // slab base (the chunk's first element)
   size_t stride;     // distance between consecutive elements of a column (complex)
@@ -155,61 +101,6 @@ template <> __device__ __forceinline__ double scale_factor<double>(double d) {
 }
 template <> __device__ __forceinline__ float scale_factor<float>(double d) { return -__frcp_rn((float)d); }
 
-template <int N, int KIND, class T>
-__device__ __forceinline__ void colpass_issue(typename C2<T>::t* buf, const ColSlab& sl) {
-  typedef typename C2<T>::t C;
-  typedef PCfg<N, T> G;
-  constexpr int CC = G::CC, NT = G::NT, LP = Pitch<CC>::value;
-  if (sl.live) {
-    const C* base = static_cast<const C*>(sl.spec);
-    for (int wi = threadIdx.x; wi < CC * N; wi += NT) {
-      const int l = wi % CC, n = wi / CC;
-      cp_async_elem(buf + n * LP + l, base + (size_t)n * sl.stride + l);
-    }
-  }
-  cp_async_commit();
-}
-
-template <int N, int KIND, class T>
-__device__ __forceinline__ void colpass_compute(typename C2<T>::t* s, const ColSlab& sl,
-                                                const typename C2<T>::t* tw) {
-  typedef typename C2<T>::t C;
-  typedef PCfg<N, T> G;
-  constexpr int CC = G::CC, NT = G::NT, LP = Pitch<CC>::value;
-  if (KIND == 0) {
-    smem_fft<N, CC, NT, -1>(s, tw);
-  } else if (KIND == 1) {
-    smem_fft<N, CC, NT, +1>(s, tw);
-  } else {
-    // forward z FFT whose last stage stores -psi/k2/(nx*ny*nz)
-    // (multi/main.f90:792, one reciprocal per mode), mode (0,0,0) and the
-    // pitch padding beyond kx = N/2 set to 0; then the inverse z FFT
-    const double nnn = (double)((long long)N * (long long)N * (long long)N);
-    const double* k2tab = sl.k2tab;
-    const double k2y = k2tab[sl.jy];
-    const int m0 = sl.m0, jy = sl.jy;
-    smem_fft_post<N, CC, NT, -1>(s, tw, [=](int n, int l, C v) {
-      const int m = m0 + l;
-      if (m > N / 2 || (m == 0 && jy == 0 && n == 0)) {
-        v.x = 0;
-        v.y = 0;
-      } else {
-        const double k2 = (k2tab[m] + k2y) + k2tab[n];
-        const T f = scale_factor<T>(k2 * nnn);
-        v.x = v.x * f;
-        v.y = v.y * f;
-      }
-      return v;
-    });
-    smem_fft<N, CC, NT, +1>(s, tw);
-  }
-  C* base = static_cast<C*>(sl.spec);
-  for (int wi = threadIdx.x; wi < CC * N; wi += NT) {
-    const int l = wi % CC, n = wi / CC;
-    base[(size_t)n * sl.stride + l] = s[n * LP + l];
-  }
-}
-
 // Slab `it` of a single simulation.
 template <int N, int KIND, class T>
 __device__ __forceinline__ ColSlab slab_single(typename C2<T>::t* spec, const void* tw, const double* k2tab,
@@ -233,74 +124,12 @@ __device__ __forceinline__ ColSlab slab_single(typename C2<T>::t* spec, const vo
   return sl;
 }
 
-// `gtw`: the launch's twiddle table (every slab of a launch shares it), copied
-// once into shared memory after the two slab buffers.
-template <int N, int KIND, class T, class Getter>
-__device__ __forceinline__ void colpass_run(int total, const typename C2<T>::t* __restrict__ gtw, Getter get) {
-  typedef typename C2<T>::t C;
-  typedef PCfg<N, T> G;
-  constexpr int LP = Pitch<G::CC>::value;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* buf0 = reinterpret_cast<C*>(smem_raw);
-  C* buf1 = buf0 + N * LP;
-  C* stw = buf1 + N * LP;
-  int it = blockIdx.x;
-  if (it >= total) return;
-  for (int q = threadIdx.x; q < N; q += G::NT) stw[q] = gtw[q];  // visible after the loop's first barrier
-  ColSlab cur = get(it);
-  colpass_issue<N, KIND, T>(buf0, cur);
-  for (int t = 0; it < total; ++t) {
-    const int nxt = it + gridDim.x;
-    ColSlab next;
-    next.live = false;
-    if (nxt < total) next = get(nxt);
-    colpass_issue<N, KIND, T>((t & 1) ? buf0 : buf1, next);
-    cp_async_wait<1>();
-    __syncthreads();
-    if (cur.live) colpass_compute<N, KIND, T>((t & 1) ? buf1 : buf0, cur, stw);
-    __syncthreads();
-    it = nxt;
-    cur = next;
-  }
-}
-
-template <int N, int KIND, class T>
-__global__ void __launch_bounds__(256, 2) colpass_kernel(typename C2<T>::t* __restrict__ spec,
-                                                     const typename C2<T>::t* __restrict__ tw,
-                                                     const double* __restrict__ k2tab, const Ctrl* __restrict__ ctrl) {
-  typedef PCfg<N, T> G;
-  colpass_run<N, KIND, T>(G::NCHUNK * N, tw,
-                          [&](int it) { return slab_single<N, KIND, T>(spec, tw, k2tab, ctrl, it); });
-}
-
-template <int N, int KIND, class T>
-__global__ void __launch_bounds__(256, 2) colpass_kernel_b(const SlotArgs<T>* __restrict__ slots, int nslots,
-                                                       int which) {
-  typedef PCfg<N, T> G;
-  const int per = G::NCHUNK * N;
-  // the class's twiddle table, from any active slot (all share it)
-  const typename C2<T>::t* tw = nullptr;
-  for (int q = 0; q < nslots && !tw; ++q)
-    if (slots[q].active) tw = (which ? slots[q].pr : slots[q].po).tw;
-  if (!tw) return;
-  colpass_run<N, KIND, T>(per * nslots, tw, [&](int it) {
-    const int sl = it / per;
-    const PoissonArgs<T>& a = which ? slots[sl].pr : slots[sl].po;
-    ColSlab s;
-    if (!slots[sl].active) {
-      s.live = false;
-      return s;
-    }
-    s = slab_single<N, KIND, T>(a.spec, a.tw, a.k2tab, a.ctrl, it - sl * per);
-    return s;
-  });
-}
-
 // ---------------------------------------------------------------- register column passes
-// Power-of-two N: the y passes and the z solve on register-resident lines
-// (reg_fft_stages).  A CTA of CC*N/8 threads holds a slab of CC kx columns;
-// thread (c, t) loads the eight elements t + (N/8)*m of column c straight
-// from HBM into registers and stores them back from registers, and in the z
+// The y passes and the z solve on register-resident lines (reg_fft_stages,
+// E = 8 elements per thread for power-of-two N, 12 for N = 3*2^k).  A CTA of
+// CC*N/E threads holds a slab of CC kx columns; thread (c, t) loads the E
+// elements t + (N/E)*m of column c straight from HBM into registers and
+// stores them back from registers, and in the z
 // solve the -1/(k^2 N^3) scaling and the first inverse stage run on the
 // registers the forward transform left.  Shared memory carries only the
 // exchanges between stages: 4 accesses per element for a y pass at 512^3
@@ -309,8 +138,8 @@ __global__ void __launch_bounds__(256, 2) colpass_kernel_b(const SlotArgs<T>* __
 // per CTA.
 template <int N, class T> struct RCfg {
   static constexpr int CC = PCfg<N, T>::CC;
-  static constexpr int NT = CC * (N / 8);
-  static constexpr bool ON = (N & (N - 1)) == 0;
+  static constexpr int E = reg_elems(N);
+  static constexpr int NT = CC * (N / E);
   // Register caps per thread (via the resident CTAs per SM the kernels are
   // built for): FP64 y passes 80 (3 CTAs of 256 threads), FP64 z solve 128
   // (a cap of 80 spilled and measured 24% slower), FP32 passes 40, 3 CTAs of
@@ -324,22 +153,25 @@ template <int N, class T> struct RCfg {
   // measured slower for the y passes and no faster for the z solve).
   static constexpr bool PF = sizeof(T) == 8;
   static constexpr bool stw(int) { return true; }
+  // (12 elements per thread: y passes 128 in FP64 and 80 in FP32, z solves
+  // 168 and 128.)
   static constexpr int minb(int kind) {
-    const int r = sizeof(T) == 8 ? (kind == 2 ? 128 : 80) : 40;
+    const int r = E == 8 ? (sizeof(T) == 8 ? (kind == 2 ? 128 : 80) : 40)
+                         : (sizeof(T) == 8 ? (kind == 2 ? 168 : 128) : (kind == 2 ? 128 : 80));
     return 65536 / (NT * r) > 1 ? 65536 / (NT * r) : 1;
   }
 };
 
 template <int N, int KIND, class T> static size_t rcolsmem() {  // exchange buffer, twiddle table, prefetch buffer
   typedef RCfg<N, T> R;
-  return ((size_t)reg_rows(N) * R::CC + (R::stw(KIND) ? N : 0) + (R::PF ? 8 * R::NT : 0)) *
+  return ((size_t)reg_rows(N) * R::CC + (R::stw(KIND) ? N : 0) + (R::PF ? R::E * R::NT : 0)) *
          sizeof(typename C2<T>::t);
 }
 
 template <int N, int KIND, class T, class Getter>
 __device__ __forceinline__ void rcol_run(int total, const typename C2<T>::t* __restrict__ gtw, Getter get) {
   typedef typename C2<T>::t C;
-  constexpr int CC = RCfg<N, T>::CC, TPC = N / 8;
+  constexpr int CC = RCfg<N, T>::CC, E = RCfg<N, T>::E, TPC = N / E;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int NT = RCfg<N, T>::NT;
   C* s = reinterpret_cast<C*>(smem_raw);
@@ -360,7 +192,7 @@ __device__ __forceinline__ void rcol_run(int total, const typename C2<T>::t* __r
     if (ps.live) {
       const C* pc = static_cast<const C*>(ps.spec) + c;
 #pragma unroll
-      for (int m = 0; m < 8; ++m) cp_async_elem(pbuf + m * NT + threadIdx.x, pc + (size_t)(t + TPC * m) * ps.stride);
+      for (int m = 0; m < E; ++m) cp_async_elem(pbuf + m * NT + threadIdx.x, pc + (size_t)(t + TPC * m) * ps.stride);
     }
     cp_async_commit();
   };
@@ -370,14 +202,14 @@ __device__ __forceinline__ void rcol_run(int total, const typename C2<T>::t* __r
     prefetch(nx);
   }
   for (int it = blockIdx.x; it < total; it += gridDim.x) {
-    C v[8];
+    C v[E];
     ColSlab sl;
     if constexpr (RCfg<N, T>::PF) {
       sl = nx;
       cp_async_wait<0>();
       if (sl.live) {
 #pragma unroll
-        for (int m = 0; m < 8; ++m) v[m] = pbuf[m * NT + threadIdx.x];
+        for (int m = 0; m < E; ++m) v[m] = pbuf[m * NT + threadIdx.x];
       }
       nx.live = false;
       if (it + (int)gridDim.x < total) nx = get(it + gridDim.x);
@@ -388,7 +220,7 @@ __device__ __forceinline__ void rcol_run(int total, const typename C2<T>::t* __r
       if (!sl.live) continue;  // the same for every thread of the CTA
       const C* lc = static_cast<const C*>(sl.spec) + c;
 #pragma unroll
-      for (int m = 0; m < 8; ++m) v[m] = lc[(size_t)(t + TPC * m) * sl.stride];
+      for (int m = 0; m < E; ++m) v[m] = lc[(size_t)(t + TPC * m) * sl.stride];
     }
     C* col = static_cast<C*>(sl.spec) + c;
     if (KIND == 0) {
@@ -405,7 +237,7 @@ __device__ __forceinline__ void rcol_run(int total, const typename C2<T>::t* __r
       const int mx = sl.m0 + c, jy = sl.jy;
       const double k2xy = k2tab[min(mx, N - 1)] + k2tab[jy];
 #pragma unroll
-      for (int m = 0; m < 8; ++m) {
+      for (int m = 0; m < E; ++m) {
         const int n = t + TPC * m;
         if (mx > N / 2 || (mx == 0 && jy == 0 && n == 0)) {
           v[m].x = 0;
@@ -420,7 +252,7 @@ __device__ __forceinline__ void rcol_run(int total, const typename C2<T>::t* __r
       reg_fft_stages<N, 1, +1>(v, s, tw, t, at);
     }
 #pragma unroll
-    for (int m = 0; m < 8; ++m) col[(size_t)(t + TPC * m) * sl.stride] = v[m];
+    for (int m = 0; m < E; ++m) col[(size_t)(t + TPC * m) * sl.stride] = v[m];
   }
 }
 
@@ -456,85 +288,9 @@ __global__ void __launch_bounds__(RCfg<N, T>::NT, RCfg<N, T>::minb(KIND)) rcol_k
   });
 }
 
-// ---------------------------------------------------------------- x inverse
-// Complex-to-real x transform of two lines at once; writes p
-// (multi/main.f90:812, 842-850: p = real(psi)).
-template <int N, class T>
-__device__ __forceinline__ void xinv_body(const typename C2<T>::t* __restrict__ spec, T* __restrict__ p,
-                                          const typename C2<T>::t* __restrict__ tw, const Ctrl* __restrict__ ctrl,
-                                          int bx, int by) {
-  typedef typename C2<T>::t C;
-  typedef PCfg<N, T> G;
-  constexpr int P = G::P, NT = G::NT;
-  if (ctrl && ctrl->status) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* s = reinterpret_cast<C*>(smem_raw);
-  constexpr int LP = Pitch<P>::value;
-  constexpr int M = N / 2 + 1;
-  const int j0 = bx * (2 * P);
-  const int k = by;
-  // Unpack two half spectra into one complex line (A + iB).
-  auto unpack = [&](int m, int q, C A, C B) {
-    if (m == 0 || m == N / 2) {
-      A.y = 0;
-      B.y = 0;
-    }
-    C z;
-    z.x = A.x - B.y;
-    z.y = A.y + B.x;
-    s[m * LP + q] = z;
-    if (m > 0 && m < N / 2) {
-      C zc;
-      zc.x = A.x + B.y;
-      zc.y = B.x - A.y;
-      s[(N - m) * LP + q] = zc;
-    }
-  };
-  if constexpr (sizeof(T) == 8) {
-    // FP64: fixed trip count, fully unrolled, every spectrum load of the
-    // thread issued before the first one is used (512^3: 0.74 -> 0.62 ms).
-    // The FP32 instantiations keep the plain loop: the same rewrite gave
-    // wrong FP32 pressures at 32^3 on B200 (cause not found), and their x
-    // passes are a small share of the FP32 step.
-    constexpr int ITERS = (P * M + NT - 1) / NT;
-    C Av[ITERS], Bv[ITERS];
-#pragma unroll
-    for (int it = 0; it < ITERS; ++it) {
-      const int wi = threadIdx.x + it * NT;
-      if (wi < P * M) {
-        const int m = wi % M, q = wi / M;
-        const C* row = spec + ((size_t)k * N + j0 + 2 * q) * G::PITCH;
-        Av[it] = row[m];
-        Bv[it] = row[G::PITCH + m];
-      }
-    }
-#pragma unroll
-    for (int it = 0; it < ITERS; ++it) {
-      const int wi = threadIdx.x + it * NT;
-      if (wi < P * M) unpack(wi % M, wi / M, Av[it], Bv[it]);
-    }
-  } else {
-    for (int wi = threadIdx.x; wi < P * M; wi += NT) {
-      const int m = wi % M, q = wi / M;
-      const C* row = spec + ((size_t)k * N + j0 + 2 * q) * G::PITCH;
-      unpack(m, q, row[m], row[G::PITCH + m]);
-    }
-  }
-  __syncthreads();
-  smem_fft<N, P, NT, +1>(s, tw);
-  for (int wi = threadIdx.x; wi < P * N; wi += NT) {
-    const int n = wi % N, q = wi / N;
-    const int ja = j0 + 2 * q;
-    const C z = s[n * LP + q];
-    p[gidx(n, ja, k, N)] = z.x;
-    p[gidx(n, ja + 1, k, N)] = z.y;
-  }
-}
-
 // ---------------------------------------------------------------- register x passes
-// Power-of-two N: the x passes on register-resident lines (reg_fft_stages),
-// P*N/8 threads per CTA, thread (q, t) holding elements t + (N/8)*m of line
-// pair q.  x inverse: each thread reads the two half spectra at
+// The x passes on register-resident lines (reg_fft_stages), P*N/E threads
+// per CTA, thread (q, t) holding elements t + (N/E)*m of line pair q.  x inverse: each thread reads the two half spectra at
 // min(n, N - n) for its own elements n straight into registers, so the
 // unpacking takes no shared-memory pass (the mirrored half reads a row
 // segment another warp reads too, an L1/L2 hit); the transformed line goes
@@ -543,8 +299,8 @@ __device__ __forceinline__ void xinv_body(const typename C2<T>::t* __restrict__ 
 // written once to shared memory for the Hermitian split, which needs modes
 // m and N - m together.
 template <int N, class T> struct XCfg {
-  static constexpr bool ON = RCfg<N, T>::ON;
-  static constexpr int NT = ON ? PCfg<N, T>::P * (N / 8) : PCfg<N, T>::NT;
+  static constexpr int E = reg_elems(N);
+  static constexpr int NT = PCfg<N, T>::P * (N / E);
   // exchange slots of a line (see reg_pad / reg_swz) and the line stride
   static constexpr int LS = sizeof(T) == 8 ? reg_rows(N) : N;
   static __device__ __forceinline__ int slot(int n) { return sizeof(T) == 8 ? reg_pad(n) : reg_swz(n); }
@@ -556,16 +312,16 @@ __device__ __forceinline__ void xinv_reg_body(const typename C2<T>::t* __restric
                                               const Ctrl* __restrict__ ctrl, int bx, int by) {
   typedef typename C2<T>::t C;
   typedef PCfg<N, T> G;
-  constexpr int TPC = N / 8;
+  constexpr int E = XCfg<N, T>::E, TPC = N / E;
   if (ctrl && ctrl->status) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* s = reinterpret_cast<C*>(smem_raw);
   const int t = threadIdx.x % TPC, q = threadIdx.x / TPC;
   const int k = by, ja = bx * (2 * G::P) + 2 * q;
   const C* row = spec + ((size_t)k * N + ja) * G::PITCH;
-  C A[8], B[8];
+  C A[E], B[E];
 #pragma unroll
-  for (int m = 0; m < 8; ++m) {
+  for (int m = 0; m < E; ++m) {
     const int n = t + TPC * m;
     const int h = (n <= N / 2) ? n : N - n;
     A[m] = row[h];
@@ -573,9 +329,9 @@ __device__ __forceinline__ void xinv_reg_body(const typename C2<T>::t* __restric
   }
   // z = A + iB on modes 0..N/2 and its Hermitian mirror above (the imaginary
   // parts of modes 0 and N/2 dropped)
-  C v[8];
+  C v[E];
 #pragma unroll
-  for (int m = 0; m < 8; ++m) {
+  for (int m = 0; m < E; ++m) {
     const int n = t + TPC * m;
     C a = A[m], b = B[m];
     if (n == 0 || n == N / 2) {
@@ -593,7 +349,7 @@ __device__ __forceinline__ void xinv_reg_body(const typename C2<T>::t* __restric
   const int base = q * XCfg<N, T>::LS;
   reg_fft_stages<N, 1, +1>(v, s, tw, t, [base](int n) { return base + XCfg<N, T>::slot(n); });
 #pragma unroll
-  for (int m = 0; m < 8; ++m) {
+  for (int m = 0; m < E; ++m) {
     const int n = t + TPC * m;
     p[gidx(n, ja, k, N)] = v[m].x;
     p[gidx(n, ja + 1, k, N)] = v[m].y;
@@ -609,16 +365,16 @@ __device__ __forceinline__ void xfwd_reg_body(const T* __restrict__ us, const T*
                                               int by) {
   typedef typename C2<T>::t C;
   typedef PCfg<N, T> G;
-  constexpr int TPC = N / 8, M = N / 2 + 1;
+  constexpr int E = XCfg<N, T>::E, TPC = N / E, M = N / 2 + 1;
   if (ctrl && ctrl->status) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* s = reinterpret_cast<C*>(smem_raw);
   const int t = threadIdx.x % TPC, q = threadIdx.x / TPC;
   const int k = by, j0 = bx * (2 * G::P);
   const int ja = j0 + 2 * q;
-  C v[8];
+  C v[E];
 #pragma unroll
-  for (int m = 0; m < 8; ++m) {
+  for (int m = 0; m < E; ++m) {
     const int n = t + TPC * m;
     v[m].x = (T)xfwd_rhs<N, MODE, T>(us, vs, ws, rhs, p0, cdiv, ddxi, n, ja, k);
     v[m].y = (T)xfwd_rhs<N, MODE, T>(us, vs, ws, rhs, p0, cdiv, ddxi, n, ja + 1, k);
@@ -627,7 +383,7 @@ __device__ __forceinline__ void xfwd_reg_body(const T* __restrict__ us, const T*
   const auto at = [base](int n) { return base + XCfg<N, T>::slot(n); };
   reg_fft_stages<N, 1, -1>(v, s, tw, t, at);
 #pragma unroll
-  for (int m = 0; m < 8; ++m) s[at(t + TPC * m)] = v[m];
+  for (int m = 0; m < E; ++m) s[at(t + TPC * m)] = v[m];
   __syncthreads();
   const T half = (T)0.5;
   for (int wi = threadIdx.x; wi < G::P * M; wi += XCfg<N, T>::NT) {
@@ -675,7 +431,7 @@ __device__ __forceinline__ void xfwd_reg_body(const T* __restrict__ us, const T*
 //     dp never goes to HBM: 32 B/pt instead of the 40 of the separate x
 //     inverse and projection.
 template <int N, class T> struct XPCfg {
-  static constexpr bool ON = RCfg<N, T>::ON && N >= 256;
+  static constexpr bool ON = (N & (N - 1)) == 0 && N >= 256;  // power-of-two sizes (8 elements per thread)
   static constexpr int P = PCfg<N, T>::P;
   static constexpr int TPC = N / 8;
   static constexpr int NT = (P + 1) * TPC;  // a multiple of 32 for N >= 256
@@ -887,78 +643,47 @@ __global__ void __launch_bounds__(XPCfg<N, T>::NT, 2) xinvproj_kernel_b(const Sl
 // ---------------------------------------------------------------- entry points
 // Single solve: block coordinates are the grid's.
 template <int N, int MODE, class T>
-__global__ void __launch_bounds__(256, 3) xfwd_kernel(const T* __restrict__ us, const T* __restrict__ vs,
+// x passes: 3 CTAs of up to 256 threads per SM with 8 elements per thread, 2
+// with 12 (their registers).
+__global__ void __launch_bounds__(256, reg_elems(N) == 8 ? 3 : 2) xfwd_kernel(const T* __restrict__ us, const T* __restrict__ vs,
                                                   const T* __restrict__ ws, const T* __restrict__ rhs,
                                                   const T* __restrict__ p0, typename C2<T>::t* __restrict__ spec,
                                                   const typename C2<T>::t* __restrict__ tw,
                                                   const Ctrl* __restrict__ ctrl, double cdiv, double ddxi) {
-  if constexpr (XCfg<N, T>::ON)
-    xfwd_reg_body<N, MODE, T>(us, vs, ws, rhs, p0, spec, tw, ctrl, cdiv, ddxi, blockIdx.x, blockIdx.y);
-  else
-    xfwd_body<N, MODE, T>(us, vs, ws, rhs, p0, spec, tw, ctrl, cdiv, ddxi, blockIdx.x, blockIdx.y);
+  xfwd_reg_body<N, MODE, T>(us, vs, ws, rhs, p0, spec, tw, ctrl, cdiv, ddxi, blockIdx.x, blockIdx.y);
 }
 template <int N, class T>
-__global__ void __launch_bounds__(256, 3) xinv_kernel(const typename C2<T>::t* __restrict__ spec, T* __restrict__ p,
+__global__ void __launch_bounds__(256, reg_elems(N) == 8 ? 3 : 2) xinv_kernel(const typename C2<T>::t* __restrict__ spec, T* __restrict__ p,
                                                   const typename C2<T>::t* __restrict__ tw,
                                                   const Ctrl* __restrict__ ctrl) {
-  if constexpr (XCfg<N, T>::ON)
-    xinv_reg_body<N, T>(spec, p, tw, ctrl, blockIdx.x, blockIdx.y);
-  else
-    xinv_body<N, T>(spec, p, tw, ctrl, blockIdx.x, blockIdx.y);
+  xinv_reg_body<N, T>(spec, p, tw, ctrl, blockIdx.x, blockIdx.y);
 }
 
 // Batched over the slots of a served ensemble: grid y = slot * N + plane.
 // `which` selects the slot's first (0) or correction (1) solve.
 template <int N, int MODE, class T>
-__global__ void __launch_bounds__(256, 3) xfwd_kernel_b(const SlotArgs<T>* __restrict__ slots, int which) {
+__global__ void __launch_bounds__(256, reg_elems(N) == 8 ? 3 : 2) xfwd_kernel_b(const SlotArgs<T>* __restrict__ slots, int which) {
   const int sl = blockIdx.y / N;
   if (!slots[sl].active) return;
   const PoissonArgs<T>& a = which ? slots[sl].pr : slots[sl].po;
-  if constexpr (XCfg<N, T>::ON)
-    xfwd_reg_body<N, MODE, T>(a.us, a.vs, a.ws, a.rhs, a.pres, a.spec, a.tw, a.ctrl, a.cdiv, a.ddxi, blockIdx.x,
-                              blockIdx.y - sl * N);
-  else
-    xfwd_body<N, MODE, T>(a.us, a.vs, a.ws, a.rhs, a.pres, a.spec, a.tw, a.ctrl, a.cdiv, a.ddxi, blockIdx.x,
-                          blockIdx.y - sl * N);
+  xfwd_reg_body<N, MODE, T>(a.us, a.vs, a.ws, a.rhs, a.pres, a.spec, a.tw, a.ctrl, a.cdiv, a.ddxi, blockIdx.x,
+                            blockIdx.y - sl * N);
 }
 template <int N, class T>
-__global__ void __launch_bounds__(256, 3) xinv_kernel_b(const SlotArgs<T>* __restrict__ slots, int which) {
+__global__ void __launch_bounds__(256, reg_elems(N) == 8 ? 3 : 2) xinv_kernel_b(const SlotArgs<T>* __restrict__ slots, int which) {
   const int sl = blockIdx.y / N;
   if (!slots[sl].active) return;
   const PoissonArgs<T>& a = which ? slots[sl].pr : slots[sl].po;
-  if constexpr (XCfg<N, T>::ON)
-    xinv_reg_body<N, T>(a.spec, a.p, a.tw, a.ctrl, blockIdx.x, blockIdx.y - sl * N);
-  else
-    xinv_body<N, T>(a.spec, a.p, a.tw, a.ctrl, blockIdx.x, blockIdx.y - sl * N);
+  xinv_reg_body<N, T>(a.spec, a.p, a.tw, a.ctrl, blockIdx.x, blockIdx.y - sl * N);
 }
 
 // ---------------------------------------------------------------- launchers
 template <int N, class T> static size_t xsmem() {
-  if constexpr (XCfg<N, T>::ON) return (size_t)PCfg<N, T>::P * XCfg<N, T>::LS * sizeof(typename C2<T>::t);
-  return (size_t)N * Pitch<PCfg<N, T>::P>::value * sizeof(typename C2<T>::t);
+  return (size_t)PCfg<N, T>::P * XCfg<N, T>::LS * sizeof(typename C2<T>::t);
 }
 
-template <int N, class T> static size_t colsmem() {  // two slab buffers + the twiddle table
-  return (2 * (size_t)N * Pitch<PCfg<N, T>::CC>::value + N) * sizeof(typename C2<T>::t);
-}
-
-// Persistent grid: resident CTAs per SM (occupancy) times the SM count.
-template <int N, int KIND, class T, bool BATCHED> static int colgrid() {
-  static int grid = 0;
-  if (!grid) {
-    int dev = 0, sms = 0, per = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (BATCHED)
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, colpass_kernel_b<N, KIND, T>, 256, colsmem<N, T>());
-    else
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, colpass_kernel<N, KIND, T>, 256, colsmem<N, T>());
-    grid = std::max(1, sms) * std::max(1, per);
-  }
-  return grid;
-}
-
-// The same for the register column passes.
+// Persistent grid of the column passes: resident CTAs per SM (occupancy)
+// times the SM count.
 template <int N, int KIND, class T, bool BATCHED> static int rcolgrid() {
   static int grid = 0;
   if (!grid) {
@@ -976,24 +701,15 @@ template <int N, int KIND, class T, bool BATCHED> static int rcolgrid() {
   return grid;
 }
 
-// Column pass KIND of one solve / of the slots of an ensemble class: the
-// register-resident transform for power-of-two N, the staged one otherwise.
+// Column pass KIND of one solve / of the slots of an ensemble class.
 template <int N, int KIND, class T> static void launch_col(const PoissonArgs<T>& a, cudaStream_t st) {
-  if constexpr (RCfg<N, T>::ON)
-    rcol_kernel<N, KIND, T><<<rcolgrid<N, KIND, T, false>(), RCfg<N, T>::NT, rcolsmem<N, KIND, T>(), st>>>(
-        a.spec, a.tw, a.k2tab, a.ctrl);
-  else
-    colpass_kernel<N, KIND, T><<<colgrid<N, KIND, T, false>(), PCfg<N, T>::NT, colsmem<N, T>(), st>>>(
-        a.spec, a.tw, a.k2tab, a.ctrl);
+  rcol_kernel<N, KIND, T><<<rcolgrid<N, KIND, T, false>(), RCfg<N, T>::NT, rcolsmem<N, KIND, T>(), st>>>(
+      a.spec, a.tw, a.k2tab, a.ctrl);
 }
 template <int N, int KIND, class T>
 static void launch_col_b(const SlotArgs<T>* slots, int nslots, int which, cudaStream_t st) {
-  if constexpr (RCfg<N, T>::ON)
-    rcol_kernel_b<N, KIND, T><<<rcolgrid<N, KIND, T, true>(), RCfg<N, T>::NT, rcolsmem<N, KIND, T>(), st>>>(
-        slots, nslots, which);
-  else
-    colpass_kernel_b<N, KIND, T><<<colgrid<N, KIND, T, true>(), PCfg<N, T>::NT, colsmem<N, T>(), st>>>(
-        slots, nslots, which);
+  rcol_kernel_b<N, KIND, T><<<rcolgrid<N, KIND, T, true>(), RCfg<N, T>::NT, rcolsmem<N, KIND, T>(), st>>>(
+      slots, nslots, which);
 }
 
 template <int N, class T> static cudaError_t set_attrs() {
@@ -1006,15 +722,7 @@ template <int N, class T> static cudaError_t set_attrs() {
   if ((e = cudaFuncSetAttribute(xfwd_kernel_b<N, 0, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, xs))) return e;
   if ((e = cudaFuncSetAttribute(xfwd_kernel_b<N, 2, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, xs))) return e;
   if ((e = cudaFuncSetAttribute(xinv_kernel_b<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, xs))) return e;
-  if constexpr (!RCfg<N, T>::ON) {
-    const int ps = (int)colsmem<N, T>();
-    if ((e = cudaFuncSetAttribute(colpass_kernel<N, 0, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps))) return e;
-    if ((e = cudaFuncSetAttribute(colpass_kernel<N, 1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps))) return e;
-    if ((e = cudaFuncSetAttribute(colpass_kernel<N, 2, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps))) return e;
-    if ((e = cudaFuncSetAttribute(colpass_kernel_b<N, 0, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps))) return e;
-    if ((e = cudaFuncSetAttribute(colpass_kernel_b<N, 1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps))) return e;
-    if ((e = cudaFuncSetAttribute(colpass_kernel_b<N, 2, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps))) return e;
-  } else {
+  {
     const int r0 = (int)rcolsmem<N, 0, T>(), r1 = (int)rcolsmem<N, 1, T>(), r2 = (int)rcolsmem<N, 2, T>();
     const cudaFuncAttribute A = cudaFuncAttributeMaxDynamicSharedMemorySize;
     if ((e = cudaFuncSetAttribute(rcol_kernel<N, 0, T>, A, r0))) return e;

@@ -1,13 +1,13 @@
 """CPU model of the register-resident FFT (reg_fft_stages in
 mhit36_b200/csrc/fft.cuh) and of the shared-memory slots its callers give it.
 
-Each thread of a line holds v[m] = x[t + (N/8)*m]; a stage with radix R and
-span NS runs butterfly b on j = t + (N/8)*b with inputs v[b + (8/R)*r],
+Each thread of a line holds E elements v[m] = x[t + (N/E)*m] (E = 8 for
+power-of-two N, 12 for N = 3*2^k); a stage with radix R (R divides E) and
+span NS runs butterfly b on j = t + (N/E)*b with inputs v[b + (E/R)*r],
 multiplies input r by w_N^(r*(j mod NS)*N/(NS*R)), and (unless it is the
 last stage) writes output r to slot at(d) with d = (j/NS)*NS*R + j%NS + r*NS,
 after which every thread reads its canonical elements back.  The model runs
-that data movement with numpy for every power-of-two size the library builds
-and checks:
+that data movement with numpy for every size the library builds and checks:
   * the result is the DFT of the line (numpy.fft), so the index maps are a
     Stockham transform;
   * every exchange slot is inside the buffer the launcher sizes, and no two
@@ -18,14 +18,18 @@ and checks:
 import numpy as np
 import pytest
 
-SIZES = (32, 64, 128, 256, 512, 1024)
+SIZES = (32, 64, 96, 128, 192, 256, 384, 512, 768, 1024)
 
 
-def pick_radix(rem):
+def reg_elems(n):
+    return 8 if n & (n - 1) == 0 else 12
+
+
+def pick_radix(rem, e):
     for r in (8, 4, 2, 3):
-        if rem % r == 0:
+        if rem % r == 0 and e % r == 0:
             return r
-    return rem
+    raise AssertionError(f"no radix for {rem} with {e} elements per thread")
 
 
 def lines_per_cta(n):
@@ -49,16 +53,17 @@ def model_fft(x, direction, at, nslots):
     -1 forward, +1 unnormalised inverse) through a shared buffer of nslots
     slots, with at(c, n) the slot of element n of line c."""
     nlines, n = x.shape
-    tpc = n // 8
+    e_ = reg_elems(n)
+    tpc = n // e_
     w = np.exp(-2j * np.pi * np.arange(n) / n)  # the twiddle table tw[m] = e^{-2 pi i m/N}
     if direction > 0:
         w = np.conj(w)
     # v[c, t, m] = x[c, t + tpc*m]
-    v = np.stack([x[:, t + tpc * np.arange(8)] for t in range(tpc)], axis=1)
+    v = np.stack([x[:, t + tpc * np.arange(e_)] for t in range(tpc)], axis=1)
     ns = 1
     while ns < n:
-        r_ = pick_radix(n // ns)
-        b_ = 8 // r_
+        r_ = pick_radix(n // ns, e_)
+        b_ = e_ // r_
         tstride = n // (ns * r_)
         out = np.empty_like(v)
         for b in range(b_):
@@ -86,13 +91,13 @@ def model_fft(x, direction, at, nslots):
                             s[slot] = v[c, t, b + b_ * r]
             for c in range(nlines):
                 for t in range(tpc):
-                    for m in range(8):
+                    for m in range(e_):
                         v[c, t, m] = s[at(c, t + tpc * m)]
         ns *= r_
     # back to line order: element t + tpc*m of line c
     y = np.empty_like(x)
     for t in range(tpc):
-        y[:, t + tpc * np.arange(8)] = v[:, t, :]
+        y[:, t + tpc * np.arange(e_)] = v[:, t, :]
     return y
 
 
@@ -134,8 +139,8 @@ def test_fused_kernel_buffers_fit(n):
     buffer ((P+1)*reg_rows(N) complex) and the previous plane's rows (2P x N)
     follow it; the whole stays inside 227 KB, and its thread count is whole
     warps (its block reduction shuffles full warps)."""
-    if n < 256:
-        pytest.skip("fused only from 256^3")
+    if n < 256 or n & (n - 1):
+        pytest.skip("fused only for power-of-two sizes from 256^3")
     p = lines_per_cta(n)
     xbytes = (p + 1) * reg_rows(n) * 16
     pbytes = (2 * p + 1) * n * 8

@@ -266,9 +266,10 @@ def test_ns_acdi_256_10_steps_every_tile_shape():
         assert abs(d["cfl"] - od["cfl"]) <= 1e-12 * abs(od["cfl"]), (kz, mty)
 
 
-@pytest.mark.parametrize("n", [256, 512])
+@pytest.mark.parametrize("n", [256, 384, 512, 768])
 def test_poisson_manufactured_large(n):
-    """sin(x)cos(2y)sin(3z) at 256^3 and 512^3 (radix plans 8x8x4 and 8x8x8)."""
+    """sin(x)cos(2y)sin(3z) at 256^3, 384^3, 512^3 and 768^3 (radix plans
+    8x8x4, 4x4x4x2x3 with 12 elements per thread, 8x8x8, 4x4x4x4x3)."""
     from mhit36_b200 import Solver
     with Solver(n, _params(grid_mode=1), phase_field=False) as s:
         x = np.arange(n) * (2 * np.pi / n)
