@@ -142,9 +142,9 @@ template <int N, class T> struct RCfg {
   static constexpr int NT = CC * (N / E);
   // Register caps per thread (via the resident CTAs per SM the kernels are
   // built for): FP64 y passes 80 (3 CTAs of 256 threads), FP64 z solve 128
-  // (a cap of 80 spilled and measured 24% slower), FP32 passes 40, 3 CTAs of
-  // 512 threads (measured on B200 at 512^3: z solve 0.68 -> 0.57 ms against no
-  // cap, y passes 0.245 -> 0.234 ms against 64).
+  // (a cap of 80 spilled and measured 24% slower), FP32 y passes 40 (3 CTAs
+  // of 512 threads; 512^3: 0.245 -> 0.234 ms against 64), FP32 z solve 64
+  // (2 CTAs; 0.537 -> 0.494 ms against 40, where it spilled).
   // FP64: the next slab is prefetched into shared memory with cp.async while
   // the current one is transformed (512^3: y passes 0.48 -> 0.41 ms, z solve
   // 0.94 -> 0.88 ms); the FP32 passes are faster without (0.24 vs 0.25 and
@@ -156,7 +156,7 @@ template <int N, class T> struct RCfg {
   // (12 elements per thread: y passes 128 in FP64 and 80 in FP32, z solves
   // 168 and 128.)
   static constexpr int minb(int kind) {
-    const int r = E == 8 ? (sizeof(T) == 8 ? (kind == 2 ? 128 : 80) : 40)
+    const int r = E == 8 ? (sizeof(T) == 8 ? (kind == 2 ? 128 : 80) : (kind == 2 ? 64 : 40))
                          : (sizeof(T) == 8 ? (kind == 2 ? 168 : 128) : (kind == 2 ? 128 : 80));
     return 65536 / (NT * r) > 1 ? 65536 / (NT * r) : 1;
   }
