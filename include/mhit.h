@@ -38,6 +38,7 @@ extern "C" {
 #define MHIT_ERR_UNSUPPORTED 7 /* grid size or option not built */
 #define MHIT_ERR_STATE 8       /* call out of order (e.g. step before set_fields) */
 #define MHIT_ERR_SCRATCH_LIMIT 9 /* grid larger than the fixed scratch of mhit_poisson_noalloc */
+#define MHIT_ERR_TIMEOUT 10      /* a kernel's bounded wait for staged data gave up */
 
 /* Field layouts for set/get. */
 #define MHIT_LAYOUT_RAW 0      /* (nx, ny, nz), the .dat interior (multi/readwrite.f90:29) */
@@ -337,6 +338,17 @@ const char* mhit_strerror(int status);
 
 /* 1 if the grid size has built kernels. */
 int mhit_size_supported(int n);
+
+/*
+ * Self-check of the bounded wait the stencil kernels use for their staged
+ * planes (tensor-map box loads completed on a shared-memory barrier): one
+ * warp arms a barrier and waits at most limit_cycles SM clock cycles.  With
+ * arrive = 1 a thread arrives and *status_out is MHIT_OK; with arrive = 0
+ * nothing arrives, the wait gives up and *status_out is MHIT_ERR_TIMEOUT,
+ * the status a step reports when a staged plane never lands.  The kernel
+ * returns either way and the CUDA context stays usable.
+ */
+int mhit_check_bounded_wait(int arrive, long long limit_cycles, int* status_out);
 
 #ifdef __cplusplus
 }

@@ -21,6 +21,7 @@ MHIT_ERR_IO = 6
 MHIT_ERR_UNSUPPORTED = 7
 MHIT_ERR_STATE = 8
 MHIT_ERR_SCRATCH_LIMIT = 9
+MHIT_ERR_TIMEOUT = 10
 MHIT_NOALLOC_MAX_N = 128
 
 MHIT_LAYOUT_RAW = 0
@@ -90,7 +91,7 @@ HEADER_SYMBOLS = [
     "mhit_step_async", "mhit_stream", "mhit_last_error", "mhit_diagnostics", "mhit_poisson_noalloc",
     "mhit_ens_create", "mhit_ens_submit", "mhit_ens_progress", "mhit_ens_wait", "mhit_ens_query", "mhit_ens_result",
     "mhit_ens_release", "mhit_ens_cancel", "mhit_ens_stats", "mhit_ens_last_error", "mhit_ens_destroy",
-    "mhit_set_tiles", "mhit_drop_count",
+    "mhit_set_tiles", "mhit_drop_count", "mhit_check_bounded_wait",
 ]
 
 _lib = None
@@ -129,6 +130,7 @@ def load_library(path: str = LIB_PATH):
         "mhit_destroy": (ctypes.c_int, [H]),
         "mhit_strerror": (ctypes.c_char_p, [ctypes.c_int]),
         "mhit_size_supported": (ctypes.c_int, [ctypes.c_int]),
+        "mhit_check_bounded_wait": (ctypes.c_int, [ctypes.c_int, ctypes.c_longlong, P(ctypes.c_int)]),
         "mhit_last_error": (ctypes.c_char_p, [H]),
         "mhit_stream": (ctypes.c_void_p, [H]),
         "mhit_profile_step": (ctypes.c_int, [H, ctypes.c_int, P(ctypes.c_double), P(ctypes.c_int)]),

@@ -452,6 +452,18 @@ void mhit_default_params(mhit_params* p) {
 
 int mhit_size_supported(int n) { return size_supported(n) ? 1 : 0; }
 
+int mhit_check_bounded_wait(int arrive, long long limit_cycles, int* status_out) {
+  if (!status_out || limit_cycles <= 0) return MHIT_ERR_INVALID;
+  int* d = nullptr;
+  if (cudaMalloc(&d, sizeof(int)) != cudaSuccess) return MHIT_ERR_NOMEM;
+  int rc = MHIT_OK;
+  if (mhit::launch_wait_check(arrive, limit_cycles, d, 0) != cudaSuccess ||
+      cudaMemcpy(status_out, d, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+    rc = MHIT_ERR_CUDA;
+  cudaFree(d);
+  return rc;
+}
+
 const char* mhit_strerror(int s) {
   switch (s) {
     case MHIT_OK: return "ok";
@@ -464,6 +476,7 @@ const char* mhit_strerror(int s) {
     case MHIT_ERR_UNSUPPORTED: return "unsupported grid size or option";
     case MHIT_ERR_STATE: return "call out of order";
     case MHIT_ERR_SCRATCH_LIMIT: return "grid larger than the fixed scratch of the allocation-free entry point";
+    case MHIT_ERR_TIMEOUT: return "a kernel's bounded wait for staged data gave up";
     default: return "unknown status";
   }
 }

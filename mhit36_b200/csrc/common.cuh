@@ -55,6 +55,53 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
+// ---- tensor-memory-accelerator tile loads completed on an mbarrier ----
+// One thread arms a ring slot's barrier with the bytes it expects and issues
+// the 2D box loads (cp.async.bulk.tensor, this GPU's own global memory, no
+// multicast); every consumer waits on the slot's phase.  The box start's
+// x coordinate times the element size must be a multiple of 16 bytes.
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* b, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(b)), "r"(count) : "memory");
+}
+// make initialised barriers visible to the async proxy (then __syncthreads)
+__device__ __forceinline__ void mbar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* b, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned long long* b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_addr(b)) : "memory");
+}
+// Wait for the phase with the given parity to complete, giving up once
+// `limit_cycles` SM clock cycles have passed (a poll may suspend the thread
+// for a short hardware time limit).  Returns false if it gave up.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* b, unsigned parity, long long limit_cycles) {
+  const unsigned a = smem_addr(b);
+  const long long t0 = clock64();
+  for (;;) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (clock64() - t0 > limit_cycles) return false;
+  }
+}
+// 2D box at (x, y) of the tensor `map` into shared memory at `dst` (16-byte
+// aligned; the box is stored densely, row pitch = box width).
+__device__ __forceinline__ void tma_load_2d(void* dst, const void* map, int x, int y, unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
+          smem_addr(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(smem_addr(bar))
+      : "memory");
+}
+
 // ---- complex helpers (double2 / float2) ----
 template <class T> struct C2;
 template <> struct C2<double> { typedef double2 t; };

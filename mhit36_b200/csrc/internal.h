@@ -110,6 +110,8 @@ cudaError_t launch_xinv_project_batched(const SlotArgs<T>* slots, int nslots, in
 // dt/rho*grad(p0 + dp) from the stored ustar, p0 and dp, into *out (one
 // double on the device; the forward-difference divergence of
 // multi/main.f90:723-725).
+// One-warp self-check of the bounded barrier wait (writes 0 or MHIT_ERR_TIMEOUT).
+cudaError_t launch_wait_check(int arrive, long long limit_cycles, int* out_dev, cudaStream_t st);
 cudaError_t launch_refine_divergence(const StencilArgs<float>& a, const float* dp, double* out, cudaStream_t st);
 // Partials the FP64 step's projection writes, and the buffer size that
 // holds either projection's partials (stride 7).

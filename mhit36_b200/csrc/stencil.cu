@@ -14,8 +14,10 @@
 // shared-memory planes, and every intermediate the reference materialises in
 // HBM (psidi, normx/y/z, rhsphi, rhsu/v/w, chempot, gradphi*, f*st) lives
 // only in shared memory or registers.
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <math.h>
+#include <string.h>
 #include "common.cuh"
 #include "internal.h"
 
@@ -144,6 +146,59 @@ __host__ __device__ constexpr int momentum_ring(int) { return 4; }
 // memory allows with ACDI (3 with 8-row tiles), 4 without; registers follow.
 __host__ __device__ constexpr int momentum_min_blocks(bool pf, int mty) { return mty == 8 ? (pf ? 3 : 4) : 2; }
 
+// Staged-plane geometry of the momentum kernel.  A staged plane is a box of
+// cells whose first column lies XS cells left of the tile, XS cells being 16
+// bytes, so that a tensor-map box load starts on a 16-byte boundary: UX x UY
+// cells for the velocities (the tile and its 1-cell ring), EX x EY for phi
+// (2-cell ring), widths rounded up to 16 bytes.  Ring slots are 128-byte
+// multiples; the slot barriers follow the force ring.
+template <class T, int TYv> struct MomGeo {
+  static constexpr int XS = 16 / (int)sizeof(T);
+  static constexpr int AL = 128 / (int)sizeof(T);
+  static constexpr int UX = (XS + TX + 1 + XS - 1) / XS * XS, UY = TYv + 2, UE = UX * UY;
+  static constexpr int EX = (XS + TX + 2 + XS - 1) / XS * XS, EY = TYv + 4, PE = EX * EY;
+  static constexpr int USL = (UE + AL - 1) / AL * AL, PSL = (PE + AL - 1) / AL * AL;
+  static constexpr int QE = (TX + 1) * (TYv + 1);
+  static __host__ __device__ constexpr size_t bar_offset(bool pf, int ns) {
+    return ((sizeof(T) * (3 * ns * USL + (pf ? ns * PSL + 6 * QE : 0))) + 7) / 8 * 8;
+  }
+  static __host__ __device__ constexpr unsigned tx_bytes(bool pf) {
+    return (unsigned)(sizeof(T) * (3 * UE + (pf ? PE : 0)));
+  }
+  // every box of the tile inside the n x n plane
+  static __host__ __device__ bool interior(int x0, int y0, int n, bool pf) {
+    const int bw = UX > EX ? UX : EX, r = pf ? 2 : 1;
+    return x0 >= XS && x0 - XS + bw <= n && y0 >= r && y0 + TYv + r <= n;
+  }
+};
+static_assert(MomGeo<double, 8>::UX == 36 && MomGeo<double, 8>::EX == 36, "FP64 staged box widths");
+static_assert(MomGeo<float, 16>::UX == 40 && MomGeo<float, 16>::EX == 40, "FP32 staged box widths");
+
+// Staged phi planes of the phase kernel: the tile and its 2-cell ring in a
+// box starting XS cells (16 bytes) left of the tile, row pitch EX.
+template <class T> struct PhaseGeo {
+  static constexpr int XS = 16 / (int)sizeof(T);
+  static constexpr int EX = (XS + TX + 2 + XS - 1) / XS * XS, EY = PTY + 4;
+  static constexpr int AL = 128 / (int)sizeof(T);
+  static constexpr int PSL = (EX * EY + AL - 1) / AL * AL;
+  static __host__ __device__ constexpr unsigned tx_bytes() { return (unsigned)(sizeof(T) * EX * EY); }
+  static __host__ __device__ bool interior(int x0, int y0, int n) {
+    return x0 >= XS && x0 - XS + EX <= n && y0 >= 2 && y0 + PTY + 2 <= n;
+  }
+};
+static_assert(PhaseGeo<double>::EX == 36 && PhaseGeo<float>::EX == 40, "staged phi box widths");
+
+// Tensor maps of the staged fields (2D views: x by y*z rows), passed to the
+// kernel as a __grid_constant__ parameter.
+struct PlaneMaps {
+  CUtensorMap u, v, w, phi;
+};
+// SM clock cycles a wait on a slot barrier lasts before it gives up (about
+// 2 s at the B200's clocks; a plane lands within microseconds), and the
+// status it records.
+constexpr long long kWaitCycles = 4000000000LL;
+constexpr int kStatusTimeout = 10;  // MHIT_ERR_TIMEOUT
+
 // 1/(sqrt(s) + tiny) for s > 0, the normalisation of A5.  With r = rsqrt(s),
 // 1/(sqrt(s) + tiny) = r/(1 + tiny*r) = r - tiny*r^2 + r*O((tiny*r)^2); the
 // first-order form is used while tiny*r < 2^-30, where the dropped term is
@@ -156,17 +211,23 @@ __device__ __forceinline__ T inv_norm_plus(T s, T tiny) {
   return (T)1 / (sqrt(s) + tiny);
 }
 
-template <class T>
-__device__ __forceinline__ void phase_body(const StencilArgs<T>& a, int KZ, int bx, int by, int bz) {
+template <class T, bool TMA>
+__device__ __forceinline__ void phase_body(const StencilArgs<T>& a, int KZ, int bx, int by, int bz,
+                                           const CUtensorMap* __restrict__ phimap) {
   if (a.ctrl->status) return;
   constexpr int TY = PTY, NT = PNT;
-  constexpr int EX = TX + 4, EY = TY + 4, PE = EX * EY;
+  // The psi ring covers the tile and its 2-cell ring (LX x EY cells); phi and
+  // psi planes are stored with row pitch EX and the ring's first column at
+  // OFF (the staged phi box starts XS cells left of the tile, 16 bytes).
+  typedef PhaseGeo<T> PG;
+  constexpr int LX = TX + 4, EY = TY + 4, PE = LX * EY, EX = PG::EX, OFF = PG::XS - 2, SL = PG::PSL;
   constexpr int FX = TX + 2, FY = TY + 2, FE = FX * FY;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   T* s_phi = reinterpret_cast<T*>(smem_raw);  // ring of 5 planes
-  T* s_psi = s_phi + 5 * PE;                  // ring of 3 planes
-  T* s_F = s_psi + 3 * PE;                    // ring of 3 planes x 3 components
+  T* s_psi = s_phi + 5 * SL;                  // ring of 3 planes
+  T* s_F = s_psi + 3 * SL;                    // ring of 3 planes x 3 components
   double* s_tab = reinterpret_cast<double*>(s_F + 9 * FE);  // log table (FP64)
+  unsigned long long* s_bar = reinterpret_cast<unsigned long long*>(s_tab + PsiMath<T>::TAB);
   for (int q = threadIdx.x; q < PsiMath<T>::TAB; q += NT) s_tab[q] = g_log_table[q];
   if (PsiMath<T>::TAB) __syncthreads();
   const int n = a.c.n;
@@ -199,19 +260,39 @@ __device__ __forceinline__ void phase_body(const StencilArgs<T>& a, int KZ, int 
 #pragma unroll
   for (int r = 0; r < NPE; ++r) {
     const int e = min(tid + r * NT, PE - 1);
-    poff[r] = wrapi(x0 - 2 + e % EX, n) + n * wrapi(y0 - 2 + e / EX, n);
+    poff[r] = wrapi(x0 - 2 + e % LX, n) + n * wrapi(y0 - 2 + e / LX, n);
   }
 #pragma unroll
   for (int r = 0; r < NFE; ++r) {
     const int e = min(tid + r * NT, FE - 1);
-    fpe[r] = (e % FX + 1) + (e / FX + 1) * EX;
+    fpe[r] = (e % FX + 1 + OFF) + (e / FX + 1) * EX;
+  }
+  // stored index of the thread's ring element r
+  const auto pidx = [&](int r) {
+    const int e = tid + r * NT;
+    if constexpr (EX == LX && OFF == 0) return e;
+    else return (e % LX + OFF) + (e / LX) * EX;
+  };
+  // Tiles whose staged phi box lies inside the grid load each plane with one
+  // tensor-map box load; the edge tiles copy their elements with cp.async
+  // and wrap.  Both fill the same stored cells.
+  const bool tma = TMA && PG::interior(x0, y0, n);
+  int sp = 3;              // ring slot of plane m at iteration m
+  unsigned bar_phase = 0;  // bit s: parity of the next phase of slot s's barrier
+  if (tma) {
+    if (tid == 0) {
+#pragma unroll
+      for (int q = 0; q < 5; ++q) mbar_init(s_bar + q, 1);
+      mbar_init_fence();
+    }
+    __syncthreads();
   }
   // Ring slots by role, rotated once per plane (no per-plane index
   // arithmetic): at iteration m the phi slots hold planes m-3 .. m+1 (m+1
   // still in flight), the psi slots m-2 .. m (m being written), and the F
   // slots m-3 .. m-1 (m-1 being written).
-  T *Phm3 = s_phi, *Phm2 = s_phi + PE, *Phm1 = s_phi + 2 * PE, *Ph0 = s_phi + 3 * PE, *Php1 = s_phi + 4 * PE;
-  T *PsW = s_psi, *Psm1 = s_psi + PE, *Psm2 = s_psi + 2 * PE;
+  T *Phm3 = s_phi, *Phm2 = s_phi + SL, *Phm1 = s_phi + 2 * SL, *Ph0 = s_phi + 3 * SL, *Php1 = s_phi + 4 * SL;
+  T *PsW = s_psi, *Psm1 = s_psi + SL, *Psm2 = s_psi + 2 * SL;
   T *FW = s_F, *Fm2 = s_F + 3 * FE, *Fm3 = s_F + 6 * FE;
   int gij[PPT], gipj[PPT], gijp[PPT];
 #pragma unroll
@@ -222,20 +303,36 @@ __device__ __forceinline__ void phase_body(const StencilArgs<T>& a, int KZ, int 
     gijp[h] = i + n * jp;
   }
 
-  // phi plane m (2-cell ring) is copied into `dst` with cp.async one
+  // phi plane m (2-cell ring) is copied into `dst` (ring slot `slot`) one
   // iteration ahead of its use.
-  auto issue = [&](T* dst, int m) {
+  auto issue = [&](T* dst, int slot, int m) {
+    if (tma) {
+      if (tid == 0) {
+        mbar_arrive_expect_tx(s_bar + slot, PG::tx_bytes());
+        tma_load_2d(dst, phimap, x0 - PG::XS, wrapi(m, n) * n + y0 - 2, s_bar + slot);
+      }
+      return;
+    }
     const T* src = a.phi_in + (size_t)wrapi(m, n) * nn;
 #pragma unroll
     for (int r = 0; r < NPE; ++r) {
       const int e = tid + r * NT;
-      if (r < NPE - 1 || e < PE) cp_async_elem(dst + e, src + poff[r]);
+      if (r < NPE - 1 || e < PE) cp_async_elem(dst + pidx(r), src + poff[r]);
     }
     cp_async_commit();
   };
-  issue(Ph0, k0 - 2);
+  issue(Ph0, sp, k0 - 2);
   for (int m = k0 - 2; m <= k0 + KZ + 1; ++m) {
-    cp_async_wait<0>();  // this thread's copies of plane m have landed
+    // plane m has landed: this thread's cp.async copies, or the slot's
+    // barrier phase for the box load (a wait that gives up records a timeout
+    // and carries on, so that no thread is left at a barrier)
+    if (tma) {
+      if (!mbar_wait(s_bar + sp, (bar_phase >> sp) & 1u, kWaitCycles)) atomicCAS(&a.ctrl->status, 0, kStatusTimeout);
+      bar_phase ^= 1u << sp;
+    } else {
+      cp_async_wait<0>();
+    }
+    const int spn = sp == 4 ? 0 : sp + 1;  // slot of plane m+1
     // velocities of the output plane k = m-2, loaded now so that their latency
     // hides behind the psi and F work below
     T uc[PPT], uxp[PPT], vc[PPT], vyp[PPT], wc[PPT], wzp[PPT];
@@ -256,8 +353,9 @@ __device__ __forceinline__ void phase_body(const StencilArgs<T>& a, int KZ, int 
     for (int r = 0; r < NPE; ++r) {
       const int e = tid + r * NT;
       if (r < NPE - 1 || e < PE) {
-        const T val = fmax(fmin(Ph0[e], (T)1), floor0);
-        PsW[e] = (val + enumv == enumv) ? psi0
+        const int ep = pidx(r);
+        const T val = fmax(fmin(Ph0[ep], (T)1), floor0);
+        PsW[ep] = (val + enumv == enumv) ? psi0
                  : ((val == (T)1) ? psi1 : eps * PsiMath<T>::log_ratio(val + enumv, (T)1 - val + enumv, s_tab));
       }
     }
@@ -265,7 +363,7 @@ __device__ __forceinline__ void phase_body(const StencilArgs<T>& a, int KZ, int 
     // the phi slot plane m+1 reuses (plane m-4, read by the last output) is
     // free.  Two barriers per plane besides the F one, not three.
     __syncthreads();
-    if (m + 1 <= k0 + KZ + 1) issue(Php1, m + 1);
+    if (m + 1 <= k0 + KZ + 1) issue(Php1, spn, m + 1);
     else cp_async_commit();
     // (2) F on plane m-1 over the tile + 1 ring.
     if (m >= k0) {
@@ -314,7 +412,7 @@ __device__ __forceinline__ void phase_body(const StencilArgs<T>& a, int KZ, int 
       const T* Fp = FW;
 #pragma unroll
       for (int h = 0; h < PPT; ++h) {
-        const int pe = (tx + 2) + (ty + h * RY + 2) * EX;
+        const int pe = (tx + 2 + OFF) + (ty + h * RY + 2) * EX;
         const int fe = (tx + 1) + (ty + h * RY + 1) * FX;
         const T c = P0[pe], pxp = P0[pe + 1], pxm = P0[pe - 1], pyp = P0[pe + EX], pym = P0[pe - EX];
         const T pzp = Pp1[pe], pzm = Pm1[pe];
@@ -337,6 +435,7 @@ __device__ __forceinline__ void phase_body(const StencilArgs<T>& a, int KZ, int 
     // ring takes the next plane
     T* t = Phm3;
     Phm3 = Phm2; Phm2 = Phm1; Phm1 = Ph0; Ph0 = Php1; Php1 = t;
+    sp = spn;
     t = Psm2;
     Psm2 = Psm1; Psm1 = PsW; PsW = t;
     t = Fm3;
@@ -351,23 +450,25 @@ __device__ __forceinline__ void phase_body(const StencilArgs<T>& a, int KZ, int 
 // and the AB2 (Euler on the first step) predictor.  Writes ustar and the new
 // rhs_o; reads the NEW phi (the reference computes B4 after A7).
 // momentum tile height: 8 or 16 rows (a tuning choice per grid size)
-template <class T, bool PF, int MTYv>
-__device__ __forceinline__ void momentum_body(const StencilArgs<T>& a, int KZ, int bx, int by, int bz) {
+template <class T, bool PF, int MTYv, bool TMA>
+__device__ __forceinline__ void momentum_body(const StencilArgs<T>& a, int KZ, int bx, int by, int bz,
+                                              const PlaneMaps* __restrict__ maps) {
   if (a.ctrl->status) return;
   // MPT output rows per thread (rows ty + 8h): 256 threads for either tile
   constexpr int TY = MTYv, MPT = MTYv / 8, NT = TX * 8;
-  constexpr int UX = TX + 2, UY = TY + 2, UE = UX * UY;  // velocity planes, 1-cell ring
-  constexpr int EX = TX + 4, EY = TY + 4, PE = EX * EY;  // phi planes, 2-cell ring
+  typedef MomGeo<T, MTYv> G;
+  constexpr int XS = G::XS, UX = G::UX, UE = G::UE, EX = G::EX, PE = G::PE;
   constexpr int QX = TX + 1, QY = TY + 1, QE = QX * QY;  // force over [-1,TX) x [-1,TY)
   // Ring of NS planes per field: planes m-2 .. m+PD at iteration m, the
   // last PD of them in flight.
   constexpr int NS = momentum_ring(MTYv), PD = NS - 3;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   T* s_u = reinterpret_cast<T*>(smem_raw);
-  T* s_v = s_u + NS * UE;
-  T* s_w = s_v + NS * UE;
-  T* s_phi = s_w + NS * UE;    // PF only
-  T* s_f = s_phi + NS * PE;    // ring of 2 planes x 3 components (PF only)
+  T* s_v = s_u + NS * G::USL;
+  T* s_w = s_v + NS * G::USL;
+  T* s_phi = s_w + NS * G::USL;  // PF only
+  T* s_f = s_phi + NS * G::PSL;  // ring of 2 planes x 3 components (PF only)
+  unsigned long long* s_bar = reinterpret_cast<unsigned long long*>(smem_raw + G::bar_offset(PF, NS));
   const int n = a.c.n;
   const T dxi = (T)a.c.dxi, ddxi = (T)a.c.ddxi, dt = (T)a.c.dt, mu_v = (T)a.c.mu, rhoi = (T)a.c.rhoi;
   const T eps = (T)a.c.eps, epsi = (T)a.c.epsi, sig6 = (T)(6.0 * a.c.sigma), lin = (T)a.c.lin_force;
@@ -380,6 +481,10 @@ __device__ __forceinline__ void momentum_body(const StencilArgs<T>& a, int KZ, i
   const size_t nn = (size_t)n * n;
   const T h = (T)0.5, q = (T)0.25;
   const T qdxi = q * dxi, hrhoi = h * rhoi;
+  // Tiles whose staged boxes lie inside the grid (no periodic wrap) load
+  // each plane with four tensor-map box loads issued by one thread; the
+  // edge tiles copy the same boxes element-wise with cp.async and wrap.
+  const bool tma = TMA && G::interior(x0, y0, n, PF);
   // Each thread owns elements tid + r*NT of the velocity, phi and force
   // planes; their in-plane offsets are the same on every plane.
   constexpr int NUE = (UE + NT - 1) / NT, NPE = (PE + NT - 1) / NT, NQE = (QE + NT - 1) / NT;
@@ -387,12 +492,12 @@ __device__ __forceinline__ void momentum_body(const StencilArgs<T>& a, int KZ, i
 #pragma unroll
   for (int r = 0; r < NUE; ++r) {
     const int e = min(tid + r * NT, UE - 1);
-    uoff[r] = wrapi(x0 - 1 + e % UX, n) + n * wrapi(y0 - 1 + e / UX, n);
+    uoff[r] = wrapi(x0 - XS + e % UX, n) + n * wrapi(y0 - 1 + e / UX, n);
   }
 #pragma unroll
   for (int r = 0; r < NPE; ++r) {
     const int e = min(tid + r * NT, PE - 1);
-    poff[r] = PF ? wrapi(x0 - 2 + e % EX, n) + n * wrapi(y0 - 2 + e / EX, n) : 0;
+    poff[r] = PF ? wrapi(x0 - XS + e % EX, n) + n * wrapi(y0 - 2 + e / EX, n) : 0;
   }
 #pragma unroll
   for (int r = 0; r < NQE; ++r) {
@@ -404,11 +509,31 @@ __device__ __forceinline__ void momentum_body(const StencilArgs<T>& a, int KZ, i
   int sl[NS];
 #pragma unroll
   for (int q2 = 0; q2 < NS; ++q2) sl[q2] = q2;
+  unsigned bar_phase = 0;  // bit s: parity of the next phase of slot s's barrier
+  if (tma) {
+    if (tid == 0) {
+#pragma unroll
+      for (int q2 = 0; q2 < NS; ++q2) mbar_init(s_bar + q2, 1);
+      mbar_init_fence();
+    }
+    __syncthreads();
+  }
 
   // Plane m of u, v, w (1-cell ring) and phi (2-cell ring) is copied into a
-  // ring slot with cp.async PD iterations ahead of its use, so the HBM
-  // latency of the planes in flight overlaps the arithmetic of plane m-1.
+  // ring slot PD iterations ahead of its use, so the HBM latency of the
+  // planes in flight overlaps the arithmetic of plane m-1.
   auto issue = [&](int slot, int m) {
+    if (tma) {
+      if (tid == 0) {
+        const int yr = wrapi(m, n) * n;
+        mbar_arrive_expect_tx(s_bar + slot, G::tx_bytes(PF));
+        tma_load_2d(s_u + slot * G::USL, &maps->u, x0 - XS, yr + y0 - 1, s_bar + slot);
+        tma_load_2d(s_v + slot * G::USL, &maps->v, x0 - XS, yr + y0 - 1, s_bar + slot);
+        tma_load_2d(s_w + slot * G::USL, &maps->w, x0 - XS, yr + y0 - 1, s_bar + slot);
+        if (PF) tma_load_2d(s_phi + slot * G::PSL, &maps->phi, x0 - XS, yr + y0 - 2, s_bar + slot);
+      }
+      return;
+    }
     const size_t zoff = (size_t)wrapi(m, n) * nn;
     const T* su = a.u + zoff;
     const T* sv = a.v + zoff;
@@ -417,9 +542,9 @@ __device__ __forceinline__ void momentum_body(const StencilArgs<T>& a, int KZ, i
     for (int r = 0; r < NUE; ++r) {
       const int e = tid + r * NT;
       if (r < NUE - 1 || e < UE) {
-        cp_async_elem(s_u + slot * UE + e, su + uoff[r]);
-        cp_async_elem(s_v + slot * UE + e, sv + uoff[r]);
-        cp_async_elem(s_w + slot * UE + e, sw + uoff[r]);
+        cp_async_elem(s_u + slot * G::USL + e, su + uoff[r]);
+        cp_async_elem(s_v + slot * G::USL + e, sv + uoff[r]);
+        cp_async_elem(s_w + slot * G::USL + e, sw + uoff[r]);
       }
     }
     if (PF) {
@@ -427,7 +552,7 @@ __device__ __forceinline__ void momentum_body(const StencilArgs<T>& a, int KZ, i
 #pragma unroll
       for (int r = 0; r < NPE; ++r) {
         const int e = tid + r * NT;
-        if (r < NPE - 1 || e < PE) cp_async_elem(s_phi + slot * PE + e, sp + poff[r]);
+        if (r < NPE - 1 || e < PE) cp_async_elem(s_phi + slot * G::PSL + e, sp + poff[r]);
       }
     }
     cp_async_commit();
@@ -439,7 +564,16 @@ __device__ __forceinline__ void momentum_body(const StencilArgs<T>& a, int KZ, i
       r_wymzp[MPT];
   bool have_prev = false;
   for (int m = k0 - 2; m <= k0 + KZ; ++m) {
-    cp_async_wait<0>();  // this thread's copies of plane m have landed
+    // plane m has landed: this thread's cp.async copies, or the slot's
+    // barrier phase for the box loads (a wait that gives up records a
+    // timeout and carries on, so that no thread is left at a barrier)
+    if (tma) {
+      const int s = sl[2];
+      if (!mbar_wait(s_bar + s, (bar_phase >> s) & 1u, kWaitCycles)) atomicCAS(&a.ctrl->status, 0, kStatusTimeout);
+      bar_phase ^= 1u << s;
+    } else {
+      cp_async_wait<0>();
+    }
     // rhs_o of the output plane k = m-1, loaded now so that its latency hides
     // behind the force computation below
     T ruo[MPT], rvo[MPT], rwo[MPT];
@@ -462,9 +596,10 @@ __device__ __forceinline__ void momentum_body(const StencilArgs<T>& a, int KZ, i
     if (PF && m >= k0) {
       // B4: chempot, grad(phi), f at plane m-1 (multi/main.f90:617-623)
       const int fm = m - 1;
-      const T* P0 = s_phi + sl[1] * PE;
-      const T* Pm = s_phi + sl[0] * PE;
-      const T* Pp = s_phi + sl[2] * PE;
+      // staged phi boxes start XS - 2 cells left of the ring
+      const T* P0 = s_phi + sl[1] * G::PSL + (XS - 2);
+      const T* Pm = s_phi + sl[0] * G::PSL + (XS - 2);
+      const T* Pp = s_phi + sl[2] * G::PSL + (XS - 2);
       T* F = s_f + ((fm + 8) & 1) * 3 * QE;
 #pragma unroll
       for (int r = 0; r < NQE; ++r) {
@@ -484,15 +619,16 @@ __device__ __forceinline__ void momentum_body(const StencilArgs<T>& a, int KZ, i
     if (PF) __syncthreads();
     if (m >= k0 + 1) {
       const int k = m - 1;
-      const T* U0 = s_u + sl[1] * UE;
-      const T* Um = s_u + sl[0] * UE;
-      const T* Up = s_u + sl[2] * UE;
-      const T* V0 = s_v + sl[1] * UE;
-      const T* Vm = s_v + sl[0] * UE;
-      const T* Vp = s_v + sl[2] * UE;
-      const T* W0 = s_w + sl[1] * UE;
-      const T* Wm = s_w + sl[0] * UE;
-      const T* Wp = s_w + sl[2] * UE;
+      // staged velocity boxes start XS - 1 cells left of the ring
+      const T* U0 = s_u + sl[1] * G::USL + (XS - 1);
+      const T* Um = s_u + sl[0] * G::USL + (XS - 1);
+      const T* Up = s_u + sl[2] * G::USL + (XS - 1);
+      const T* V0 = s_v + sl[1] * G::USL + (XS - 1);
+      const T* Vm = s_v + sl[0] * G::USL + (XS - 1);
+      const T* Vp = s_v + sl[2] * G::USL + (XS - 1);
+      const T* W0 = s_w + sl[1] * G::USL + (XS - 1);
+      const T* Wm = s_w + sl[0] * G::USL + (XS - 1);
+      const T* Wp = s_w + sl[2] * G::USL + (XS - 1);
 #pragma unroll
       for (int hh = 0; hh < MPT; ++hh) {
         const int j = y0 + ty + 8 * hh;
@@ -862,12 +998,14 @@ __device__ __forceinline__ void finalize_body(const double* __restrict__ partial
 // ============================================================ entry points
 // Single simulation: block coordinates are the grid's.
 template <class T>
-__global__ void __launch_bounds__(PNT, phase_min_blocks<T>()) phase_kernel(StencilArgs<T> a, int KZ) {
-  phase_body<T>(a, KZ, blockIdx.x, blockIdx.y, blockIdx.z);
+__global__ void __launch_bounds__(PNT, phase_min_blocks<T>())
+    phase_kernel(StencilArgs<T> a, int KZ, const __grid_constant__ CUtensorMap phimap) {
+  phase_body<T, true>(a, KZ, blockIdx.x, blockIdx.y, blockIdx.z, &phimap);
 }
 template <class T, bool PF, int MTYv>
-__global__ void __launch_bounds__(TX * 8, momentum_min_blocks(PF, MTYv)) momentum_kernel(StencilArgs<T> a, int KZ) {
-  momentum_body<T, PF, MTYv>(a, KZ, blockIdx.x, blockIdx.y, blockIdx.z);
+__global__ void __launch_bounds__(TX * 8, momentum_min_blocks(PF, MTYv))
+    momentum_kernel(StencilArgs<T> a, int KZ, const __grid_constant__ PlaneMaps maps) {
+  momentum_body<T, PF, MTYv, true>(a, KZ, blockIdx.x, blockIdx.y, blockIdx.z, &maps);
 }
 template <class T, int PKZ>
 __global__ void __launch_bounds__(NT, 4) project_kernel(StencilArgs<T> a) {
@@ -893,7 +1031,7 @@ __global__ void __launch_bounds__(PNT, phase_min_blocks<T>()) phase_kernel_b(con
   const int par = (int)(a.ctrl->nstep & 1);
   a.phi_in = slots[sl].phi[par];
   a.phi_out = slots[sl].phi[par ^ 1];
-  phase_body<T>(a, KZ, blockIdx.x, blockIdx.y, blockIdx.z - sl * zch);
+  phase_body<T, false>(a, KZ, blockIdx.x, blockIdx.y, blockIdx.z - sl * zch, nullptr);
 }
 template <class T, bool PF, int MTYv>
 __global__ void __launch_bounds__(TX * 8, momentum_min_blocks(PF, MTYv)) momentum_kernel_b(const SlotArgs<T>* __restrict__ slots, int KZ,
@@ -902,7 +1040,7 @@ __global__ void __launch_bounds__(TX * 8, momentum_min_blocks(PF, MTYv)) momentu
   if (!slots[sl].active) return;
   StencilArgs<T> a = slots[sl].st;
   if (PF) a.phi_in = slots[sl].phi[(int)((a.ctrl->nstep + 1) & 1)];  // the updated phi
-  momentum_body<T, PF, MTYv>(a, KZ, blockIdx.x, blockIdx.y, blockIdx.z - sl * zch);
+  momentum_body<T, PF, MTYv, false>(a, KZ, blockIdx.x, blockIdx.y, blockIdx.z - sl * zch, nullptr);
 }
 template <class T, int PKZ>
 __global__ void __launch_bounds__(NT, 4) project_kernel_b(const SlotArgs<T>* __restrict__ slots, int zch) {
@@ -921,6 +1059,23 @@ __global__ void __launch_bounds__(FNT) finalize_kernel_b(const SlotArgs<T>* __re
   const int sl = blockIdx.x;
   if (!slots[sl].active) return;
   finalize_body(slots[sl].st.partials, nparts, stride, slots[sl].st.ctrl, slots[sl].st.c);
+}
+
+// Self-check of the bounded slot-barrier wait the staged-plane kernels use:
+// one warp arms a barrier; if `arrive`, a thread arrives on it, otherwise
+// nothing does and the wait gives up after `limit` cycles.  Writes 0 or the
+// timeout status; the kernel returns either way.
+__global__ void wait_check_kernel(int arrive, long long limit, int* out) {
+  __shared__ unsigned long long bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_init_fence();
+  }
+  __syncthreads();
+  if (arrive && threadIdx.x == 0) mbar_arrive(&bar);
+  const bool ok = mbar_wait(&bar, 0, limit);
+  __syncwarp();
+  if (threadIdx.x == 0) *out = ok ? 0 : kStatusTimeout;
 }
 
 // u -= mean in place, then mean = 0 (materialises the lazy mean removal).
@@ -942,13 +1097,56 @@ __global__ void clear_mean_kernel(Ctrl* ctrl) {
 
 // ============================================================ launchers
 template <class T> static size_t phase_smem() {
-  return sizeof(T) * (size_t)(8 * (TX + 4) * (PTY + 4) + 9 * (TX + 2) * (PTY + 2)) + sizeof(double) * PsiMath<T>::TAB;
+  return sizeof(T) * (size_t)(8 * PhaseGeo<T>::PSL + 9 * (TX + 2) * (PTY + 2)) +
+         sizeof(double) * (PsiMath<T>::TAB + 5);
 }
 template <class T> static size_t momentum_smem(bool pf, int mty) {
   const int ns = momentum_ring(mty);
-  size_t s = 3 * ns * (TX + 2) * (mty + 2);
-  if (pf) s += ns * (TX + 4) * (mty + 4) + 2 * 3 * (TX + 1) * (mty + 1);
-  return sizeof(T) * s;
+  const size_t b = mty == 8 ? MomGeo<T, 8>::bar_offset(pf, ns) : MomGeo<T, 16>::bar_offset(pf, ns);
+  return b + sizeof(unsigned long long) * ns;
+}
+
+// cuTensorMapEncodeTiled from the driver, resolved once through the runtime
+// (no link-time dependency on the driver library).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<EncodeTiledFn>(p);
+  }();
+  return fn;
+}
+
+// 2D map of an n^3 field as n columns by n*n rows, box bw x bh.
+template <class T> static cudaError_t plane_map(CUtensorMap* m, const T* base, int n, int bw, int bh) {
+  EncodeTiledFn fn = encode_tiled();
+  if (!fn) return cudaErrorNotSupported;
+  const cuuint64_t dims[2] = {(cuuint64_t)n, (cuuint64_t)n * n};
+  const cuuint64_t strides[1] = {(cuuint64_t)n * sizeof(T)};
+  const cuuint32_t box[2] = {(cuuint32_t)bw, (cuuint32_t)bh};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = fn(m, sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+                        const_cast<T*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+template <class T, int TYv> static cudaError_t momentum_maps(PlaneMaps* pm, const StencilArgs<T>& a, bool pf) {
+  typedef MomGeo<T, TYv> G;
+  const int n = a.c.n;
+  cudaError_t e;
+  if ((e = plane_map(&pm->u, a.u, n, G::UX, G::UY))) return e;
+  if ((e = plane_map(&pm->v, a.v, n, G::UX, G::UY))) return e;
+  if ((e = plane_map(&pm->w, a.w, n, G::UX, G::UY))) return e;
+  if (pf && (e = plane_map(&pm->phi, a.phi_in, n, G::EX, G::EY))) return e;
+  return cudaSuccess;
 }
 
 int stencil_size_ok(int n) {
@@ -988,7 +1186,10 @@ template <class T> cudaError_t launch_phase(const StencilArgs<T>& a, cudaStream_
   const int n = a.c.n;
   if (kz <= 0) kz = pick_kz(n);
   dim3 grid(n / TX, n / PTY, n / kz);
-  phase_kernel<T><<<grid, PNT, phase_smem<T>(), st>>>(a, kz);
+  CUtensorMap pm;
+  cudaError_t e = plane_map(&pm, a.phi_in, n, PhaseGeo<T>::EX, PTY + 4);
+  if (e) return e;
+  phase_kernel<T><<<grid, PNT, phase_smem<T>(), st>>>(a, kz, pm);
   return cudaGetLastError();
 }
 
@@ -998,12 +1199,16 @@ template <class T> cudaError_t launch_momentum(const StencilArgs<T>& a, bool pf,
   if (mty != 8) mty = 16;
   dim3 grid(n / TX, n / mty, n / kz);
   const size_t sm = momentum_smem<T>(pf, mty);
+  PlaneMaps pm;
+  memset(&pm, 0, sizeof(pm));
+  cudaError_t e = mty == 8 ? momentum_maps<T, 8>(&pm, a, pf) : momentum_maps<T, 16>(&pm, a, pf);
+  if (e) return e;
   if (mty == 8) {
-    if (pf) momentum_kernel<T, true, 8><<<grid, TX * 8, sm, st>>>(a, kz);
-    else momentum_kernel<T, false, 8><<<grid, TX * 8, sm, st>>>(a, kz);
+    if (pf) momentum_kernel<T, true, 8><<<grid, TX * 8, sm, st>>>(a, kz, pm);
+    else momentum_kernel<T, false, 8><<<grid, TX * 8, sm, st>>>(a, kz, pm);
   } else {
-    if (pf) momentum_kernel<T, true, 16><<<grid, TX * 8, sm, st>>>(a, kz);
-    else momentum_kernel<T, false, 16><<<grid, TX * 8, sm, st>>>(a, kz);
+    if (pf) momentum_kernel<T, true, 16><<<grid, TX * 8, sm, st>>>(a, kz, pm);
+    else momentum_kernel<T, false, 16><<<grid, TX * 8, sm, st>>>(a, kz, pm);
   }
   return cudaGetLastError();
 }
@@ -1042,6 +1247,11 @@ template <class T> cudaError_t launch_materialize(T* u, T* v, T* w, int n, Ctrl*
 }
 
 int stencil_kz_ok(int n, int kz) { return kz >= 2 && kz <= n && n % kz == 0; }
+
+cudaError_t launch_wait_check(int arrive, long long limit_cycles, int* out_dev, cudaStream_t st) {
+  wait_check_kernel<<<1, 32, 0, st>>>(arrive, limit_cycles, out_dev);
+  return cudaGetLastError();
+}
 
 template <class T>
 cudaError_t launch_phase_batched(const SlotArgs<T>* slots, int nslots, int n, int kz, cudaStream_t st) {

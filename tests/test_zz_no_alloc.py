@@ -16,7 +16,7 @@ pytestmark = pytest.mark.gpu
 
 TOL = 1e-13  # the Poisson tolerance of tests/test_gpu_parity.py
 
-# largest first; 96 exercises the radix-3 (staged shared-memory) transform
+# largest first; 96 exercises the mixed-radix (radix-3) register transform
 CASES = [(128, 1, 1), (96, 0, 1), (64, 0, 0), (32, 1, 0)]
 
 
