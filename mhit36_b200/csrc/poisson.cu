@@ -642,10 +642,14 @@ __global__ void __launch_bounds__(XPCfg<N, T>::NT, 2) xinvproj_kernel_b(const Sl
 
 // ---------------------------------------------------------------- entry points
 // Single solve: block coordinates are the grid's.
-template <int N, int MODE, class T>
 // x passes: 3 CTAs of up to 256 threads per SM with 8 elements per thread, 2
-// with 12 (their registers).
-__global__ void __launch_bounds__(256, reg_elems(N) == 8 ? 3 : 2) xfwd_kernel(const T* __restrict__ us, const T* __restrict__ vs,
+// with 12 (their registers); 4 for the FP32 divergence pass (64 registers,
+// no spill: 0.469 -> 0.446 ms at 512^3 on B200).
+template <int N, int MODE, class T> __host__ __device__ constexpr int xfwd_min_blocks() {
+  return reg_elems(N) == 8 ? (sizeof(T) == 4 && MODE != 2 ? 4 : 3) : 2;
+}
+template <int N, int MODE, class T>
+__global__ void __launch_bounds__(256, xfwd_min_blocks<N, MODE, T>()) xfwd_kernel(const T* __restrict__ us, const T* __restrict__ vs,
                                                   const T* __restrict__ ws, const T* __restrict__ rhs,
                                                   const T* __restrict__ p0, typename C2<T>::t* __restrict__ spec,
                                                   const typename C2<T>::t* __restrict__ tw,
@@ -662,7 +666,7 @@ __global__ void __launch_bounds__(256, reg_elems(N) == 8 ? 3 : 2) xinv_kernel(co
 // Batched over the slots of a served ensemble: grid y = slot * N + plane.
 // `which` selects the slot's first (0) or correction (1) solve.
 template <int N, int MODE, class T>
-__global__ void __launch_bounds__(256, reg_elems(N) == 8 ? 3 : 2) xfwd_kernel_b(const SlotArgs<T>* __restrict__ slots, int which) {
+__global__ void __launch_bounds__(256, xfwd_min_blocks<N, MODE, T>()) xfwd_kernel_b(const SlotArgs<T>* __restrict__ slots, int which) {
   const int sl = blockIdx.y / N;
   if (!slots[sl].active) return;
   const PoissonArgs<T>& a = which ? slots[sl].pr : slots[sl].po;
