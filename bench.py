@@ -61,7 +61,7 @@ ALGO_BYTES_STEP = {"fp64": {True: 280, False: 232}, "fp32": {True: 200, False: 1
 # profiles/kernels_fp64_256_full.md).  A stencil or column pass touches every
 # point the same way at any size, so traffic scales with the points
 # processed; a full 512^3 capture is too large to take under ncu.
-DRAM_BYTES_PER_POINT_FP64 = {"momentum": 103.86, "phase": 40.18, "project": 54.13, "xfwd": 30.80,
+DRAM_BYTES_PER_POINT_FP64 = {"momentum": 103.45, "phase": 40.25, "project": 54.13, "xfwd": 30.80,
                              "yfwd": 13.59, "zsolve": 13.64, "yinv": 13.59, "xinv": 13.82, "xinvproj": 55.30}
 
 
@@ -455,22 +455,30 @@ def main():
         # CUDA events on the solver's stream bracket the whole job: the uploads
         # and downloads run on that stream, and every host pause between its
         # operations shows as stream idle time inside the span
-        f0 = torch.cuda.Event(enable_timing=True)
-        f1 = torch.cuda.Event(enable_timing=True)
+        f0, fa, fb, f1 = (torch.cuda.Event(enable_timing=True) for _ in range(4))
         f0.record(stream)
         s.set_fields_ptr(*ptr)
+        fa.record(stream)
         for _ in range(args.steps):
             s.step(1)  # returns the step's diagnostics to the host
+        fb.record(stream)
         s.get_fields_ptr(*ptr)
         f1.record(stream)
         f1.synchronize()
         torch.cuda.synchronize()
         el = max_over_ranks(f0.elapsed_time(f1) / 1e3, world)
         nf = len(hb)
+        # where the time goes: the upload, the steps (each one waits for its
+        # diagnostics on the host, so the gap to the device-timed step is the
+        # cost of that synchronisation), the download
+        steps_ms = fa.elapsed_time(fb) / args.steps
         e2e = {"value": replicas_rate(world, npts, args.steps, el), "unit": UNIT,
                "h2d_bytes_per_step": nf * npts * 8 / args.steps,
                "d2h_bytes_per_step": nf * npts * 8 / args.steps + 88,
-               "ms_per_step": el / args.steps * 1e3}
+               "ms_per_step": el / args.steps * 1e3,
+               "upload_ms": round(f0.elapsed_time(fa), 3), "download_ms": round(fb.elapsed_time(f1), 3),
+               "step_with_diag_readback_ms": round(steps_ms, 4),
+               "diag_sync_overhead_ms": round(steps_ms - step_ms, 4)}
 
     mem_bytes = s.memory_bytes()
     s.close()
