@@ -60,6 +60,11 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
 // the 2D box loads (cp.async.bulk.tensor, this GPU's own global memory, no
 // multicast); every consumer waits on the slot's phase.  The box start's
 // x coordinate times the element size must be a multiple of 16 bytes.
+// SM clock cycles a wait on a ring slot's barrier lasts before it gives up
+// (about 2 s at the B200's clocks; a staged plane lands within microseconds),
+// and the sticky status it records.
+constexpr long long kWaitCycles = 4000000000LL;
+constexpr int kStatusTimeout = 10;  // MHIT_ERR_TIMEOUT
 __device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void mbar_init(unsigned long long* b, unsigned count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(b)), "r"(count) : "memory");
@@ -99,6 +104,15 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const void* map, int x, i
       "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
           smem_addr(dst)),
       "l"(map), "r"(x), "r"(y), "r"(smem_addr(bar))
+      : "memory");
+}
+
+// 3D box at (x, y, z) of the tensor `map` into shared memory at `dst`.
+__device__ __forceinline__ void tma_load_3d(void* dst, const void* map, int x, int y, int z, unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];\n" ::"r"(smem_addr(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_addr(bar))
       : "memory");
 }
 

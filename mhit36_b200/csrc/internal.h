@@ -1,7 +1,9 @@
 // Internal launcher interface between the C ABI (capi.cu) and the kernels.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stddef.h>
+#include <stdint.h>
 #include "common.cuh"
 
 // Grid sizes with built kernels (N^3 cells, N a multiple of 32 with radices 2/3).
@@ -110,6 +112,10 @@ cudaError_t launch_xinv_project_batched(const SlotArgs<T>* slots, int nslots, in
 // dt/rho*grad(p0 + dp) from the stored ustar, p0 and dp, into *out (one
 // double on the device; the forward-difference divergence of
 // multi/main.f90:723-725).
+// Tensor map of 8-byte elements (tiled, no swizzle): dims innermost first,
+// strides[rank-1] in bytes, box per dim.
+cudaError_t encode_tensor_map(CUtensorMap* m, int rank, const void* base, const uint64_t* dims,
+                              const uint64_t* strides, const uint32_t* box);
 // One-warp self-check of the bounded barrier wait (writes 0 or MHIT_ERR_TIMEOUT).
 cudaError_t launch_wait_check(int arrive, long long limit_cycles, int* out_dev, cudaStream_t st);
 cudaError_t launch_refine_divergence(const StencilArgs<float>& a, const float* dp, double* out, cudaStream_t st);

@@ -20,6 +20,7 @@
 #include <algorithm>
 #include "common.cuh"
 #include "fft.cuh"
+#include <string.h>
 #include "internal.h"
 
 namespace mhit {
@@ -78,6 +79,7 @@ struct ColSlab {
   const double* k2tab;
   int jy;            // z solve: the ky index of the slab
   int m0;            // z solve: first kx of the chunk
+  int chunk, line;   // the slab's column chunk and line (y pass: kz; z solve: ky)
   bool live;         // false: skip (inactive slot or stopped simulation)
 };
 
@@ -108,6 +110,8 @@ __device__ __forceinline__ ColSlab slab_single(typename C2<T>::t* spec, const vo
   typedef PCfg<N, T> G;
   ColSlab sl;
   const int chunk = it % G::NCHUNK, line = it / G::NCHUNK;
+  sl.chunk = chunk;
+  sl.line = line;
   sl.live = !(ctrl && ctrl->status);
   sl.tw = tw;
   sl.k2tab = k2tab;
@@ -145,10 +149,13 @@ template <int N, class T> struct RCfg {
   // (a cap of 80 spilled and measured 24% slower), FP32 y passes 40 (3 CTAs
   // of 512 threads; 512^3: 0.245 -> 0.234 ms against 64), FP32 z solve 64
   // (2 CTAs; 0.537 -> 0.494 ms against 40, where it spilled).
-  // FP64: the next slab is prefetched into shared memory with cp.async while
-  // the current one is transformed (512^3: y passes 0.48 -> 0.41 ms, z solve
-  // 0.94 -> 0.88 ms); the FP32 passes are faster without (0.24 vs 0.25 and
-  // 0.56 vs 0.66 ms), their extra buffer costing resident CTAs.  The twiddle
+  // FP64: the next slab is prefetched into shared memory while the current
+  // one is transformed (512^3: y passes 0.48 -> 0.41 ms, z solve 0.94 ->
+  // 0.88 ms with per-element cp.async; one thread issuing tensor-map box
+  // loads instead: y passes 0.42 -> 0.40 ms, z solve 0.86 -> 0.76 ms); the
+  // FP32 passes are faster without (0.24 vs 0.25 and 0.56 vs 0.66 ms),
+  // their extra buffer costing resident CTAs.  The served ensemble's batched
+  // passes, whose spectra differ per slot, keep the cp.async prefetch.  The twiddle
   // table sits in shared memory for every pass (reading it through L1
   // measured slower for the y passes and no faster for the z solve).
   static constexpr bool PF = sizeof(T) == 8;
@@ -162,22 +169,39 @@ template <int N, class T> struct RCfg {
   }
 };
 
+// Rows of a prefetch box (the slab's N lines in N/BH boxes of at most 256).
+template <int N> __host__ __device__ constexpr int rcol_box_rows() { return N <= 256 ? N : (N % 256 == 0 ? 256 : N / 2); }
+
 template <int N, int KIND, class T> static size_t rcolsmem() {  // exchange buffer, twiddle table, prefetch buffer
   typedef RCfg<N, T> R;
-  return ((size_t)reg_rows(N) * R::CC + (R::stw(KIND) ? N : 0) + (R::PF ? R::E * R::NT : 0)) *
-         sizeof(typename C2<T>::t);
+  // prefetch buffer rounded to a 128-byte boundary, then its barrier
+  const size_t head = ((size_t)reg_rows(N) * R::CC + (R::stw(KIND) ? N : 0)) * sizeof(typename C2<T>::t);
+  if (!R::PF) return head;
+  return (head + 127) / 128 * 128 + (size_t)R::E * R::NT * sizeof(typename C2<T>::t) + 8;
 }
 
-template <int N, int KIND, class T, class Getter>
-__device__ __forceinline__ void rcol_run(int total, const typename C2<T>::t* __restrict__ gtw, Getter get) {
+template <int N, int KIND, class T, bool TMA, class Getter>
+__device__ __forceinline__ void rcol_run(int total, const typename C2<T>::t* __restrict__ gtw, Getter get,
+                                         const CUtensorMap* map, Ctrl* ctrl) {
   typedef typename C2<T>::t C;
   constexpr int CC = RCfg<N, T>::CC, E = RCfg<N, T>::E, TPC = N / E;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   constexpr int NT = RCfg<N, T>::NT;
   C* s = reinterpret_cast<C*>(smem_raw);
   C* stw = s + reg_rows(N) * CC;
-  C* pbuf = stw + (RCfg<N, T>::stw(KIND) ? N : 0);
+  constexpr size_t HEAD = ((size_t)reg_rows(N) * CC + (RCfg<N, T>::stw(KIND) ? N : 0)) * sizeof(C);
+  C* pbuf = reinterpret_cast<C*>(smem_raw + (RCfg<N, T>::PF ? (HEAD + 127) / 128 * 128 : HEAD));
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(pbuf + E * NT);
   if ((int)blockIdx.x >= total) return;
+  if constexpr (TMA) {
+    if (threadIdx.x == 0) {
+      mbar_init(bar, 1);
+      mbar_init_fence();
+    }
+    __syncthreads();
+  }
+  unsigned phase = 0;
+  bool pend = false;  // a box load of the next slab is in flight (the same in every thread)
   const C* tw = gtw;
   if constexpr (RCfg<N, T>::stw(KIND)) {
     for (int q = threadIdx.x; q < N; q += NT) stw[q] = gtw[q];
@@ -188,13 +212,32 @@ __device__ __forceinline__ void rcol_run(int total, const typename C2<T>::t* __r
   const auto at = [c](int n) { return reg_pad(n) * CC + c; };
   // prefetch: each thread copies its own eight elements of the next slab into
   // its own slots (m*NT + tid), so only its own cp.async wait orders them
+  // (TMA: one thread loads the whole slab, N/BH boxes of CC columns x BH
+  // lines, into the same cells: element (line n, column c) at n*CC + c)
   auto prefetch = [&](const ColSlab& ps) {
-    if (ps.live) {
-      const C* pc = static_cast<const C*>(ps.spec) + c;
+    if constexpr (TMA) {
+      if (ps.live) {
+        if (threadIdx.x == 0) {
+          constexpr int BH = rcol_box_rows<N>();
+          mbar_arrive_expect_tx(bar, (unsigned)(E * NT * sizeof(C)));
+          const int x = ps.chunk * CC * 2;
 #pragma unroll
-      for (int m = 0; m < E; ++m) cp_async_elem(pbuf + m * NT + threadIdx.x, pc + (size_t)(t + TPC * m) * ps.stride);
+          for (int b = 0; b < N / BH; ++b) {
+            if (KIND == 2) tma_load_3d(pbuf + b * BH * CC, map, x, ps.line, b * BH, bar);
+            else tma_load_2d(pbuf + b * BH * CC, map, x, ps.line * N + b * BH, bar);
+          }
+        }
+        pend = true;
+      }
+    } else {
+      if (ps.live) {
+        const C* pc = static_cast<const C*>(ps.spec) + c;
+#pragma unroll
+        for (int m = 0; m < E; ++m)
+          cp_async_elem(pbuf + m * NT + threadIdx.x, pc + (size_t)(t + TPC * m) * ps.stride);
+      }
+      cp_async_commit();
     }
-    cp_async_commit();
   };
   ColSlab nx;
   if constexpr (RCfg<N, T>::PF) {
@@ -206,13 +249,22 @@ __device__ __forceinline__ void rcol_run(int total, const typename C2<T>::t* __r
     ColSlab sl;
     if constexpr (RCfg<N, T>::PF) {
       sl = nx;
-      cp_async_wait<0>();
+      if constexpr (TMA) {
+        if (pend) {
+          if (!mbar_wait(bar, phase, kWaitCycles) && ctrl) atomicCAS(&ctrl->status, 0, kStatusTimeout);
+          phase ^= 1u;
+          pend = false;
+        }
+      } else {
+        cp_async_wait<0>();
+      }
       if (sl.live) {
 #pragma unroll
         for (int m = 0; m < E; ++m) v[m] = pbuf[m * NT + threadIdx.x];
       }
       nx.live = false;
       if (it + (int)gridDim.x < total) nx = get(it + gridDim.x);
+      if constexpr (TMA) __syncthreads();  // every thread has read the buffer the next box fills
       prefetch(nx);
       if (!sl.live) continue;
     } else {
@@ -260,10 +312,12 @@ template <int N, int KIND, class T>
 __global__ void __launch_bounds__(RCfg<N, T>::NT, RCfg<N, T>::minb(KIND)) rcol_kernel(typename C2<T>::t* __restrict__ spec,
                                                               const typename C2<T>::t* __restrict__ tw,
                                                               const double* __restrict__ k2tab,
-                                                              const Ctrl* __restrict__ ctrl) {
+                                                              const Ctrl* __restrict__ ctrl,
+                                                              const __grid_constant__ CUtensorMap map) {
   typedef PCfg<N, T> G;
-  rcol_run<N, KIND, T>(G::NCHUNK * N, tw,
-                       [&](int it) { return slab_single<N, KIND, T>(spec, tw, k2tab, ctrl, it); });
+  rcol_run<N, KIND, T, RCfg<N, T>::PF>(G::NCHUNK * N, tw,
+                                       [&](int it) { return slab_single<N, KIND, T>(spec, tw, k2tab, ctrl, it); },
+                                       &map, const_cast<Ctrl*>(ctrl));
 }
 
 template <int N, int KIND, class T>
@@ -275,7 +329,7 @@ __global__ void __launch_bounds__(RCfg<N, T>::NT, RCfg<N, T>::minb(KIND)) rcol_k
   for (int q = 0; q < nslots && !tw; ++q)
     if (slots[q].active) tw = (which ? slots[q].pr : slots[q].po).tw;
   if (!tw) return;
-  rcol_run<N, KIND, T>(per * nslots, tw, [&](int it) {
+  rcol_run<N, KIND, T, false>(per * nslots, tw, [&](int it) {
     const int sl = it / per;
     const PoissonArgs<T>& a = which ? slots[sl].pr : slots[sl].po;
     ColSlab s;
@@ -285,7 +339,7 @@ __global__ void __launch_bounds__(RCfg<N, T>::NT, RCfg<N, T>::minb(KIND)) rcol_k
     }
     s = slab_single<N, KIND, T>(a.spec, a.tw, a.k2tab, a.ctrl, it - sl * per);
     return s;
-  });
+  }, nullptr, nullptr);
 }
 
 // ---------------------------------------------------------------- register x passes
@@ -314,7 +368,7 @@ __device__ __forceinline__ void xinv_reg_body(const typename C2<T>::t* __restric
   typedef PCfg<N, T> G;
   constexpr int E = XCfg<N, T>::E, TPC = N / E;
   if (ctrl && ctrl->status) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   C* s = reinterpret_cast<C*>(smem_raw);
   const int t = threadIdx.x % TPC, q = threadIdx.x / TPC;
   const int k = by, ja = bx * (2 * G::P) + 2 * q;
@@ -367,7 +421,7 @@ __device__ __forceinline__ void xfwd_reg_body(const T* __restrict__ us, const T*
   typedef PCfg<N, T> G;
   constexpr int E = XCfg<N, T>::E, TPC = N / E, M = N / 2 + 1;
   if (ctrl && ctrl->status) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   C* s = reinterpret_cast<C*>(smem_raw);
   const int t = threadIdx.x % TPC, q = threadIdx.x / TPC;
   const int k = by, j0 = bx * (2 * G::P);
@@ -454,7 +508,7 @@ __device__ __forceinline__ void xinvproj_body(const typename C2<T>::t* __restric
   constexpr size_t PITCH = PCfg<N, T>::PITCH;
   static_assert(NT % 32 == 0, "whole warps");
   if (a.ctrl->status) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   C* sx = reinterpret_cast<C*>(smem_raw);
   double* sp = reinterpret_cast<double*>(smem_raw);  // the plane's p rows, after its transform
   double* spp = reinterpret_cast<double*>(smem_raw + X::ABYTES);  // the previous plane's rows
@@ -706,9 +760,35 @@ template <int N, int KIND, class T, bool BATCHED> static int rcolgrid() {
 }
 
 // Column pass KIND of one solve / of the slots of an ensemble class.
+// FP64: a tensor map of the half spectrum as doubles, (2*PITCH, N*N rows)
+// for the y passes and (2*PITCH, N, N) for the z solve, boxes of CC columns
+// by BH lines.
 template <int N, int KIND, class T> static void launch_col(const PoissonArgs<T>& a, cudaStream_t st) {
+  typedef PCfg<N, T> G;
+  CUtensorMap map;
+  memset(&map, 0, sizeof(map));
+  if constexpr (RCfg<N, T>::PF) {
+    const uint64_t row = (uint64_t)G::PITCH * sizeof(typename C2<T>::t);
+    const uint32_t bh = (uint32_t)rcol_box_rows<N>(), bw = (uint32_t)(2 * G::CC);
+    cudaError_t e;
+    if (KIND == 2) {
+      const uint64_t dims[3] = {(uint64_t)2 * G::PITCH, (uint64_t)N, (uint64_t)N};
+      const uint64_t strides[2] = {row, row * N};
+      const uint32_t box[3] = {bw, 1, bh};
+      e = encode_tensor_map(&map, 3, a.spec, dims, strides, box);
+    } else {
+      const uint64_t dims[2] = {(uint64_t)2 * G::PITCH, (uint64_t)N * N};
+      const uint64_t strides[1] = {row};
+      const uint32_t box[2] = {bw, bh};
+      e = encode_tensor_map(&map, 2, a.spec, dims, strides, box);
+    }
+    if (e) {  // surfaces as the launch error of an empty grid
+      rcol_kernel<N, KIND, T><<<0, 1, 0, st>>>(a.spec, a.tw, a.k2tab, a.ctrl, map);
+      return;
+    }
+  }
   rcol_kernel<N, KIND, T><<<rcolgrid<N, KIND, T, false>(), RCfg<N, T>::NT, rcolsmem<N, KIND, T>(), st>>>(
-      a.spec, a.tw, a.k2tab, a.ctrl);
+      a.spec, a.tw, a.k2tab, a.ctrl, map);
 }
 template <int N, int KIND, class T>
 static void launch_col_b(const SlotArgs<T>* slots, int nslots, int which, cudaStream_t st) {

@@ -197,11 +197,6 @@ static_assert(PhaseGeo<double>::EX == 36 && PhaseGeo<float>::EX == 40, "staged p
 struct PlaneMaps {
   CUtensorMap u, v, w, phi;
 };
-// SM clock cycles a wait on a slot barrier lasts before it gives up (about
-// 2 s at the B200's clocks; a plane lands within microseconds), and the
-// status it records.
-constexpr long long kWaitCycles = 4000000000LL;
-constexpr int kStatusTimeout = 10;  // MHIT_ERR_TIMEOUT
 
 // 1/(sqrt(s) + tiny) for s > 0, the normalisation of A5.  With r = rsqrt(s),
 // 1/(sqrt(s) + tiny) = r/(1 + tiny*r) = r - tiny*r^2 + r*O((tiny*r)^2); the
@@ -1125,6 +1120,24 @@ static EncodeTiledFn encode_tiled() {
     return reinterpret_cast<EncodeTiledFn>(p);
   }();
   return fn;
+}
+
+cudaError_t encode_tensor_map(CUtensorMap* m, int rank, const void* base, const uint64_t* dims,
+                              const uint64_t* strides, const uint32_t* box) {
+  EncodeTiledFn fn = encode_tiled();
+  if (!fn) return cudaErrorNotSupported;
+  if (rank < 1 || rank > 3) return cudaErrorInvalidValue;
+  cuuint64_t d[3], sb[2];
+  cuuint32_t bx[3], estr[3] = {1, 1, 1};
+  for (int i = 0; i < rank; ++i) {
+    d[i] = dims[i];
+    bx[i] = box[i];
+    if (i + 1 < rank) sb[i] = strides[i];
+  }
+  const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, (cuuint32_t)rank, const_cast<void*>(base), d, sb, bx, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
 // 2D map of an n^3 field as n columns by n*n rows, box bw x bh.
