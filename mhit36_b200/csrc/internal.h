@@ -115,7 +115,7 @@ cudaError_t launch_xinv_project_batched(const SlotArgs<T>* slots, int nslots, in
 // Tensor map of 8-byte elements (tiled, no swizzle): dims innermost first,
 // strides[rank-1] in bytes, box per dim.
 cudaError_t encode_tensor_map(CUtensorMap* m, int rank, const void* base, const uint64_t* dims,
-                              const uint64_t* strides, const uint32_t* box);
+                              const uint64_t* strides, const uint32_t* box, int elem_bytes = 8);
 // One-warp self-check of the bounded barrier wait (writes 0 or MHIT_ERR_TIMEOUT).
 cudaError_t launch_wait_check(int arrive, long long limit_cycles, int* out_dev, cudaStream_t st);
 cudaError_t launch_refine_divergence(const StencilArgs<float>& a, const float* dp, double* out, cudaStream_t st);

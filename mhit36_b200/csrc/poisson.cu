@@ -159,6 +159,10 @@ template <int N, class T> struct RCfg {
   // table sits in shared memory for every pass (reading it through L1
   // measured slower for the y passes and no faster for the z solve).
   static constexpr bool PF = sizeof(T) == 8;
+  // single solves: the prefetch arrives by tensor-map box loads; the FP32 z
+  // solve takes it too (0.495 -> 0.438 ms at 512^3), the FP32 y passes do
+  // not (0.235 -> 0.248 ms)
+  static constexpr bool pf_single(int kind) { return sizeof(T) == 8 || kind == 2; }
   static constexpr bool stw(int) { return true; }
   // (12 elements per thread: y passes 128 in FP64 and 80 in FP32, z solves
   // 168 and 128.)
@@ -172,15 +176,16 @@ template <int N, class T> struct RCfg {
 // Rows of a prefetch box (the slab's N lines in N/BH boxes of at most 256).
 template <int N> __host__ __device__ constexpr int rcol_box_rows() { return N <= 256 ? N : (N % 256 == 0 ? 256 : N / 2); }
 
-template <int N, int KIND, class T> static size_t rcolsmem() {  // exchange buffer, twiddle table, prefetch buffer
+template <int N, int KIND, class T, bool PF = RCfg<N, T>::PF>
+static size_t rcolsmem() {  // exchange buffer, twiddle table, prefetch buffer
   typedef RCfg<N, T> R;
   // prefetch buffer rounded to a 128-byte boundary, then its barrier
   const size_t head = ((size_t)reg_rows(N) * R::CC + (R::stw(KIND) ? N : 0)) * sizeof(typename C2<T>::t);
-  if (!R::PF) return head;
+  if (!PF) return head;
   return (head + 127) / 128 * 128 + (size_t)R::E * R::NT * sizeof(typename C2<T>::t) + 8;
 }
 
-template <int N, int KIND, class T, bool TMA, class Getter>
+template <int N, int KIND, class T, bool PF, bool TMA, class Getter>
 __device__ __forceinline__ void rcol_run(int total, const typename C2<T>::t* __restrict__ gtw, Getter get,
                                          const CUtensorMap* map, Ctrl* ctrl) {
   typedef typename C2<T>::t C;
@@ -190,7 +195,7 @@ __device__ __forceinline__ void rcol_run(int total, const typename C2<T>::t* __r
   C* s = reinterpret_cast<C*>(smem_raw);
   C* stw = s + reg_rows(N) * CC;
   constexpr size_t HEAD = ((size_t)reg_rows(N) * CC + (RCfg<N, T>::stw(KIND) ? N : 0)) * sizeof(C);
-  C* pbuf = reinterpret_cast<C*>(smem_raw + (RCfg<N, T>::PF ? (HEAD + 127) / 128 * 128 : HEAD));
+  C* pbuf = reinterpret_cast<C*>(smem_raw + (PF ? (HEAD + 127) / 128 * 128 : HEAD));
   unsigned long long* bar = reinterpret_cast<unsigned long long*>(pbuf + E * NT);
   if ((int)blockIdx.x >= total) return;
   if constexpr (TMA) {
@@ -240,14 +245,14 @@ __device__ __forceinline__ void rcol_run(int total, const typename C2<T>::t* __r
     }
   };
   ColSlab nx;
-  if constexpr (RCfg<N, T>::PF) {
+  if constexpr (PF) {
     nx = get(blockIdx.x);
     prefetch(nx);
   }
   for (int it = blockIdx.x; it < total; it += gridDim.x) {
     C v[E];
     ColSlab sl;
-    if constexpr (RCfg<N, T>::PF) {
+    if constexpr (PF) {
       sl = nx;
       if constexpr (TMA) {
         if (pend) {
@@ -315,7 +320,8 @@ __global__ void __launch_bounds__(RCfg<N, T>::NT, RCfg<N, T>::minb(KIND)) rcol_k
                                                               const Ctrl* __restrict__ ctrl,
                                                               const __grid_constant__ CUtensorMap map) {
   typedef PCfg<N, T> G;
-  rcol_run<N, KIND, T, RCfg<N, T>::PF>(G::NCHUNK * N, tw,
+  constexpr bool PFS = RCfg<N, T>::pf_single(KIND);
+  rcol_run<N, KIND, T, PFS, PFS>(G::NCHUNK * N, tw,
                                        [&](int it) { return slab_single<N, KIND, T>(spec, tw, k2tab, ctrl, it); },
                                        &map, const_cast<Ctrl*>(ctrl));
 }
@@ -329,7 +335,7 @@ __global__ void __launch_bounds__(RCfg<N, T>::NT, RCfg<N, T>::minb(KIND)) rcol_k
   for (int q = 0; q < nslots && !tw; ++q)
     if (slots[q].active) tw = (which ? slots[q].pr : slots[q].po).tw;
   if (!tw) return;
-  rcol_run<N, KIND, T, false>(per * nslots, tw, [&](int it) {
+  rcol_run<N, KIND, T, RCfg<N, T>::PF, false>(per * nslots, tw, [&](int it) {
     const int sl = it / per;
     const PoissonArgs<T>& a = which ? slots[sl].pr : slots[sl].po;
     ColSlab s;
@@ -753,21 +759,21 @@ template <int N, int KIND, class T, bool BATCHED> static int rcolgrid() {
                                                     rcolsmem<N, KIND, T>());
     else
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, rcol_kernel<N, KIND, T>, RCfg<N, T>::NT,
-                                                    rcolsmem<N, KIND, T>());
+                                                    rcolsmem<N, KIND, T, RCfg<N, T>::pf_single(KIND)>());
     grid = std::max(1, sms) * std::max(1, per);
   }
   return grid;
 }
 
 // Column pass KIND of one solve / of the slots of an ensemble class.
-// FP64: a tensor map of the half spectrum as doubles, (2*PITCH, N*N rows)
-// for the y passes and (2*PITCH, N, N) for the z solve, boxes of CC columns
-// by BH lines.
+// Where the single solve prefetches (pf_single): a tensor map of the half
+// spectrum as reals, (2*PITCH, N*N rows) for the y passes and (2*PITCH, N,
+// N) for the z solve, boxes of CC columns by BH lines.
 template <int N, int KIND, class T> static void launch_col(const PoissonArgs<T>& a, cudaStream_t st) {
   typedef PCfg<N, T> G;
   CUtensorMap map;
   memset(&map, 0, sizeof(map));
-  if constexpr (RCfg<N, T>::PF) {
+  if constexpr (RCfg<N, T>::pf_single(KIND)) {
     const uint64_t row = (uint64_t)G::PITCH * sizeof(typename C2<T>::t);
     const uint32_t bh = (uint32_t)rcol_box_rows<N>(), bw = (uint32_t)(2 * G::CC);
     cudaError_t e;
@@ -775,20 +781,21 @@ template <int N, int KIND, class T> static void launch_col(const PoissonArgs<T>&
       const uint64_t dims[3] = {(uint64_t)2 * G::PITCH, (uint64_t)N, (uint64_t)N};
       const uint64_t strides[2] = {row, row * N};
       const uint32_t box[3] = {bw, 1, bh};
-      e = encode_tensor_map(&map, 3, a.spec, dims, strides, box);
+      e = encode_tensor_map(&map, 3, a.spec, dims, strides, box, (int)sizeof(T));
     } else {
       const uint64_t dims[2] = {(uint64_t)2 * G::PITCH, (uint64_t)N * N};
       const uint64_t strides[1] = {row};
       const uint32_t box[2] = {bw, bh};
-      e = encode_tensor_map(&map, 2, a.spec, dims, strides, box);
+      e = encode_tensor_map(&map, 2, a.spec, dims, strides, box, (int)sizeof(T));
     }
     if (e) {  // surfaces as the launch error of an empty grid
       rcol_kernel<N, KIND, T><<<0, 1, 0, st>>>(a.spec, a.tw, a.k2tab, a.ctrl, map);
       return;
     }
   }
-  rcol_kernel<N, KIND, T><<<rcolgrid<N, KIND, T, false>(), RCfg<N, T>::NT, rcolsmem<N, KIND, T>(), st>>>(
-      a.spec, a.tw, a.k2tab, a.ctrl, map);
+  rcol_kernel<N, KIND, T><<<rcolgrid<N, KIND, T, false>(), RCfg<N, T>::NT,
+                             rcolsmem<N, KIND, T, RCfg<N, T>::pf_single(KIND)>(), st>>>(a.spec, a.tw, a.k2tab, a.ctrl,
+                                                                                       map);
 }
 template <int N, int KIND, class T>
 static void launch_col_b(const SlotArgs<T>* slots, int nslots, int which, cudaStream_t st) {
@@ -809,9 +816,12 @@ template <int N, class T> static cudaError_t set_attrs() {
   {
     const int r0 = (int)rcolsmem<N, 0, T>(), r1 = (int)rcolsmem<N, 1, T>(), r2 = (int)rcolsmem<N, 2, T>();
     const cudaFuncAttribute A = cudaFuncAttributeMaxDynamicSharedMemorySize;
-    if ((e = cudaFuncSetAttribute(rcol_kernel<N, 0, T>, A, r0))) return e;
-    if ((e = cudaFuncSetAttribute(rcol_kernel<N, 1, T>, A, r1))) return e;
-    if ((e = cudaFuncSetAttribute(rcol_kernel<N, 2, T>, A, r2))) return e;
+    const int q0 = (int)rcolsmem<N, 0, T, RCfg<N, T>::pf_single(0)>(),
+              q1 = (int)rcolsmem<N, 1, T, RCfg<N, T>::pf_single(1)>(),
+              q2 = (int)rcolsmem<N, 2, T, RCfg<N, T>::pf_single(2)>();
+    if ((e = cudaFuncSetAttribute(rcol_kernel<N, 0, T>, A, q0))) return e;
+    if ((e = cudaFuncSetAttribute(rcol_kernel<N, 1, T>, A, q1))) return e;
+    if ((e = cudaFuncSetAttribute(rcol_kernel<N, 2, T>, A, q2))) return e;
     if ((e = cudaFuncSetAttribute(rcol_kernel_b<N, 0, T>, A, r0))) return e;
     if ((e = cudaFuncSetAttribute(rcol_kernel_b<N, 1, T>, A, r1))) return e;
     if ((e = cudaFuncSetAttribute(rcol_kernel_b<N, 2, T>, A, r2))) return e;

@@ -1123,7 +1123,7 @@ static EncodeTiledFn encode_tiled() {
 }
 
 cudaError_t encode_tensor_map(CUtensorMap* m, int rank, const void* base, const uint64_t* dims,
-                              const uint64_t* strides, const uint32_t* box) {
+                              const uint64_t* strides, const uint32_t* box, int elem_bytes) {
   EncodeTiledFn fn = encode_tiled();
   if (!fn) return cudaErrorNotSupported;
   if (rank < 1 || rank > 3) return cudaErrorInvalidValue;
@@ -1134,7 +1134,7 @@ cudaError_t encode_tensor_map(CUtensorMap* m, int rank, const void* base, const 
     bx[i] = box[i];
     if (i + 1 < rank) sb[i] = strides[i];
   }
-  const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, (cuuint32_t)rank, const_cast<void*>(base), d, sb, bx, estr,
+  const CUresult r = fn(m, elem_bytes == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, (cuuint32_t)rank, const_cast<void*>(base), d, sb, bx, estr,
                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
