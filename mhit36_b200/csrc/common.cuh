@@ -97,6 +97,15 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* b, unsigned parity
     if (clock64() - t0 > limit_cycles) return false;
   }
 }
+// Tensor maps in global memory written by a kernel (generic proxy): the
+// writer releases them to the tensor-map proxy, the thread that issues
+// box loads with one acquires it first.
+__device__ __forceinline__ void tensormap_release() {
+  asm volatile("fence.proxy.tensormap::generic.release.gpu;\n" ::: "memory");
+}
+__device__ __forceinline__ void tensormap_acquire(const void* map) {
+  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(map) : "memory");
+}
 // 2D box at (x, y) of the tensor `map` into shared memory at `dst` (16-byte
 // aligned; the box is stored densely, row pitch = box width).
 __device__ __forceinline__ void tma_load_2d(void* dst, const void* map, int x, int y, unsigned long long* bar) {

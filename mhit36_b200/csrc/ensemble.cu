@@ -383,12 +383,14 @@ int fail(mhit_ensemble* e, cudaError_t err, const char* where) {
   } while (0)
 
 // Slot-table writes in stream order: the entry travels as a kernel argument,
-// so no host buffer has to outlive the call.
+// so no host buffer has to outlive the call.  The entry holds the slot's
+// tensor maps, so the writes are released to the tensor-map proxy.
 template <class T>
-__global__ void slot_write_kernel(SlotArgs<T>* __restrict__ dst, SlotArgs<T> val) {
+__global__ void slot_write_kernel(SlotArgs<T>* __restrict__ dst, const __grid_constant__ SlotArgs<T> val) {
   const int* s = reinterpret_cast<const int*>(&val);
   int* d = reinterpret_cast<int*>(dst);
   for (int q = threadIdx.x; q < (int)(sizeof(SlotArgs<T>) / sizeof(int)); q += blockDim.x) d[q] = s[q];
+  mhit::tensormap_release();
 }
 
 template <class T>
@@ -497,13 +499,17 @@ template <class T> SlotArgs<T> build_args(Class* c, SlotBuf& b, const StepConst&
   return a;
 }
 
-// Write slot s's table entry (the request's buffers and constants) on the class stream.
+// Write slot s's table entry (the request's buffers, constants and tensor
+// maps) on the class stream.
 cudaError_t write_entry(Class* c, int s, const StepConst& k, int active) {
+  cudaError_t e;
   if (c->precision == MHIT_FP64) {
     c->hd[s] = build_args<double>(c, c->slots[s], k, active);
+    if ((e = mhit::encode_slot_maps<double>(&c->hd[s], c->n, c->pf != 0))) return e;
     slot_write_kernel<double><<<1, 64, 0, c->st>>>(static_cast<SlotArgs<double>*>(c->d_slots) + s, c->hd[s]);
   } else {
     c->hf[s] = build_args<float>(c, c->slots[s], k, active);
+    if ((e = mhit::encode_slot_maps<float>(&c->hf[s], c->n, c->pf != 0))) return e;
     slot_write_kernel<float><<<1, 64, 0, c->st>>>(static_cast<SlotArgs<float>*>(c->d_slots) + s, c->hf[s]);
   }
   return cudaGetLastError();

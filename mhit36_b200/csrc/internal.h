@@ -56,6 +56,22 @@ template <class T> struct StencilArgs {
   StepConst c;
 };
 
+// Tensor maps of the momentum kernel's staged fields (2D views of an n^3
+// field: x by y*z rows).
+struct PlaneMaps {
+  CUtensorMap u, v, w, phi;
+};
+// Tensor maps of a served-ensemble slot, kept in its device table entry:
+// the momentum kernel's boxes per tile height (8, 16) and phi parity, the
+// phase kernel's phi box per parity, and the column passes' spectrum views
+// (y passes, z solve).  Written by a kernel, so readers acquire them through
+// the tensor-map proxy before use.
+struct SlotMaps {
+  PlaneMaps mom[2][2];
+  CUtensorMap phase_phi[2];
+  CUtensorMap col_y, col_z;
+};
+
 // One resident simulation of a served ensemble: the batched kernels read
 // their arguments from a device array of these, one per slot of a class.
 template <class T> struct SlotArgs {
@@ -66,6 +82,7 @@ template <class T> struct SlotArgs {
   float* dp;            // FP32 form: correction pressure
   int active;           // 0: every kernel of this slot returns at once
   int pad_;
+  SlotMaps maps;        // tensor maps of this slot's fields (encoded on the host)
 };
 
 // Batched launches over `nslots` slots of one class (grid size n).  kz is
@@ -116,6 +133,10 @@ cudaError_t launch_xinv_project_batched(const SlotArgs<T>* slots, int nslots, in
 // strides[rank-1] in bytes, box per dim.
 cudaError_t encode_tensor_map(CUtensorMap* m, int rank, const void* base, const uint64_t* dims,
                               const uint64_t* strides, const uint32_t* box, int elem_bytes = 8);
+// A slot's tensor maps from its table entry's field pointers (n^3 grid).
+template <class T> cudaError_t encode_slot_maps(SlotArgs<T>* a, int n, bool phase_field);
+// The column passes' spectrum views of a slot (part of encode_slot_maps).
+template <class T> cudaError_t encode_column_maps(SlotMaps* m, const void* spec, int n);
 // One-warp self-check of the bounded barrier wait (writes 0 or MHIT_ERR_TIMEOUT).
 cudaError_t launch_wait_check(int arrive, long long limit_cycles, int* out_dev, cudaStream_t st);
 cudaError_t launch_refine_divergence(const StencilArgs<float>& a, const float* dp, double* out, cudaStream_t st);

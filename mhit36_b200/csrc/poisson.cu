@@ -81,6 +81,9 @@ struct ColSlab {
   int m0;            // z solve: first kx of the chunk
   int chunk, line;   // the slab's column chunk and line (y pass: kz; z solve: ky)
   bool live;         // false: skip (inactive slot or stopped simulation)
+  bool gmap;         // map lives in an ensemble slot table (acquire it first)
+  const CUtensorMap* map;  // the spectrum view the prefetch boxes come from
+  Ctrl* ctrl;        // where a prefetch wait that gives up records the timeout
 };
 
 // The z solve's per-mode factor -1/(k^2 nx ny nz) (multi/main.f90:792), for
@@ -112,6 +115,9 @@ __device__ __forceinline__ ColSlab slab_single(typename C2<T>::t* spec, const vo
   const int chunk = it % G::NCHUNK, line = it / G::NCHUNK;
   sl.chunk = chunk;
   sl.line = line;
+  sl.gmap = false;
+  sl.map = nullptr;
+  sl.ctrl = const_cast<Ctrl*>(ctrl);
   sl.live = !(ctrl && ctrl->status);
   sl.tw = tw;
   sl.k2tab = k2tab;
@@ -149,19 +155,16 @@ template <int N, class T> struct RCfg {
   // (a cap of 80 spilled and measured 24% slower), FP32 y passes 40 (3 CTAs
   // of 512 threads; 512^3: 0.245 -> 0.234 ms against 64), FP32 z solve 64
   // (2 CTAs; 0.537 -> 0.494 ms against 40, where it spilled).
-  // FP64: the next slab is prefetched into shared memory while the current
-  // one is transformed (512^3: y passes 0.48 -> 0.41 ms, z solve 0.94 ->
-  // 0.88 ms with per-element cp.async; one thread issuing tensor-map box
-  // loads instead: y passes 0.42 -> 0.40 ms, z solve 0.86 -> 0.76 ms); the
-  // FP32 passes are faster without (0.24 vs 0.25 and 0.56 vs 0.66 ms),
-  // their extra buffer costing resident CTAs.  The served ensemble's batched
-  // passes, whose spectra differ per slot, keep the cp.async prefetch.  The twiddle
-  // table sits in shared memory for every pass (reading it through L1
-  // measured slower for the y passes and no faster for the z solve).
-  static constexpr bool PF = sizeof(T) == 8;
-  // single solves: the prefetch arrives by tensor-map box loads; the FP32 z
-  // solve takes it too (0.495 -> 0.438 ms at 512^3), the FP32 y passes do
-  // not (0.235 -> 0.248 ms)
+  // The next slab is prefetched into shared memory while the current one is
+  // transformed, by one thread issuing tensor-map box loads (the single
+  // solve's map is a kernel parameter, an ensemble slot's sits in its table
+  // entry).  FP64 (512^3): y passes 0.48 -> 0.41 ms and z solve 0.94 ->
+  // 0.88 ms with per-element cp.async, 0.42 -> 0.40 and 0.86 -> 0.76 ms with
+  // the box loads instead.  FP32: the z solve 0.495 -> 0.438 ms with the box
+  // loads; the y passes run without a prefetch (0.235 against 0.248 ms with
+  // it).  The twiddle table sits in shared memory for every pass (reading it
+  // through L1 measured slower for the y passes and no faster for the z
+  // solve).
   static constexpr bool pf_single(int kind) { return sizeof(T) == 8 || kind == 2; }
   static constexpr bool stw(int) { return true; }
   // (12 elements per thread: y passes 128 in FP64 and 80 in FP32, z solves
@@ -176,7 +179,7 @@ template <int N, class T> struct RCfg {
 // Rows of a prefetch box (the slab's N lines in N/BH boxes of at most 256).
 template <int N> __host__ __device__ constexpr int rcol_box_rows() { return N <= 256 ? N : (N % 256 == 0 ? 256 : N / 2); }
 
-template <int N, int KIND, class T, bool PF = RCfg<N, T>::PF>
+template <int N, int KIND, class T, bool PF = RCfg<N, T>::pf_single(KIND)>
 static size_t rcolsmem() {  // exchange buffer, twiddle table, prefetch buffer
   typedef RCfg<N, T> R;
   // prefetch buffer rounded to a 128-byte boundary, then its barrier
@@ -187,7 +190,7 @@ static size_t rcolsmem() {  // exchange buffer, twiddle table, prefetch buffer
 
 template <int N, int KIND, class T, bool PF, bool TMA, class Getter>
 __device__ __forceinline__ void rcol_run(int total, const typename C2<T>::t* __restrict__ gtw, Getter get,
-                                         const CUtensorMap* map, Ctrl* ctrl) {
+                                         int = 0) {
   typedef typename C2<T>::t C;
   constexpr int CC = RCfg<N, T>::CC, E = RCfg<N, T>::E, TPC = N / E;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -224,6 +227,8 @@ __device__ __forceinline__ void rcol_run(int total, const typename C2<T>::t* __r
       if (ps.live) {
         if (threadIdx.x == 0) {
           constexpr int BH = rcol_box_rows<N>();
+          const CUtensorMap* map = ps.map;
+          if (ps.gmap) tensormap_acquire(map);
           mbar_arrive_expect_tx(bar, (unsigned)(E * NT * sizeof(C)));
           const int x = ps.chunk * CC * 2;
 #pragma unroll
@@ -256,7 +261,7 @@ __device__ __forceinline__ void rcol_run(int total, const typename C2<T>::t* __r
       sl = nx;
       if constexpr (TMA) {
         if (pend) {
-          if (!mbar_wait(bar, phase, kWaitCycles) && ctrl) atomicCAS(&ctrl->status, 0, kStatusTimeout);
+          if (!mbar_wait(bar, phase, kWaitCycles) && sl.ctrl) atomicCAS(&sl.ctrl->status, 0, kStatusTimeout);
           phase ^= 1u;
           pend = false;
         }
@@ -321,9 +326,11 @@ __global__ void __launch_bounds__(RCfg<N, T>::NT, RCfg<N, T>::minb(KIND)) rcol_k
                                                               const __grid_constant__ CUtensorMap map) {
   typedef PCfg<N, T> G;
   constexpr bool PFS = RCfg<N, T>::pf_single(KIND);
-  rcol_run<N, KIND, T, PFS, PFS>(G::NCHUNK * N, tw,
-                                       [&](int it) { return slab_single<N, KIND, T>(spec, tw, k2tab, ctrl, it); },
-                                       &map, const_cast<Ctrl*>(ctrl));
+  rcol_run<N, KIND, T, PFS, PFS>(G::NCHUNK * N, tw, [&](int it) {
+    ColSlab s = slab_single<N, KIND, T>(spec, tw, k2tab, ctrl, it);
+    s.map = &map;
+    return s;
+  });
 }
 
 template <int N, int KIND, class T>
@@ -335,7 +342,8 @@ __global__ void __launch_bounds__(RCfg<N, T>::NT, RCfg<N, T>::minb(KIND)) rcol_k
   for (int q = 0; q < nslots && !tw; ++q)
     if (slots[q].active) tw = (which ? slots[q].pr : slots[q].po).tw;
   if (!tw) return;
-  rcol_run<N, KIND, T, RCfg<N, T>::PF, false>(per * nslots, tw, [&](int it) {
+  constexpr bool PFS = RCfg<N, T>::pf_single(KIND);
+  rcol_run<N, KIND, T, PFS, PFS>(per * nslots, tw, [&](int it) {
     const int sl = it / per;
     const PoissonArgs<T>& a = which ? slots[sl].pr : slots[sl].po;
     ColSlab s;
@@ -344,8 +352,10 @@ __global__ void __launch_bounds__(RCfg<N, T>::NT, RCfg<N, T>::minb(KIND)) rcol_k
       return s;
     }
     s = slab_single<N, KIND, T>(a.spec, a.tw, a.k2tab, a.ctrl, it - sl * per);
+    s.map = KIND == 2 ? &slots[sl].maps.col_z : &slots[sl].maps.col_y;
+    s.gmap = true;
     return s;
-  }, nullptr, nullptr);
+  });
 }
 
 // ---------------------------------------------------------------- register x passes
@@ -769,33 +779,35 @@ template <int N, int KIND, class T, bool BATCHED> static int rcolgrid() {
 // Where the single solve prefetches (pf_single): a tensor map of the half
 // spectrum as reals, (2*PITCH, N*N rows) for the y passes and (2*PITCH, N,
 // N) for the z solve, boxes of CC columns by BH lines.
-template <int N, int KIND, class T> static void launch_col(const PoissonArgs<T>& a, cudaStream_t st) {
+// The spectrum view column pass KIND prefetches from (where it prefetches):
+// the half spectrum as reals, (2*PITCH, N*N rows) for the y passes and
+// (2*PITCH, N, N) for the z solve, boxes of CC columns by BH lines.
+template <int N, int KIND, class T> static cudaError_t col_map(CUtensorMap* map, const void* spec) {
   typedef PCfg<N, T> G;
-  CUtensorMap map;
-  memset(&map, 0, sizeof(map));
-  if constexpr (RCfg<N, T>::pf_single(KIND)) {
-    const uint64_t row = (uint64_t)G::PITCH * sizeof(typename C2<T>::t);
-    const uint32_t bh = (uint32_t)rcol_box_rows<N>(), bw = (uint32_t)(2 * G::CC);
-    cudaError_t e;
-    if (KIND == 2) {
-      const uint64_t dims[3] = {(uint64_t)2 * G::PITCH, (uint64_t)N, (uint64_t)N};
-      const uint64_t strides[2] = {row, row * N};
-      const uint32_t box[3] = {bw, 1, bh};
-      e = encode_tensor_map(&map, 3, a.spec, dims, strides, box, (int)sizeof(T));
-    } else {
-      const uint64_t dims[2] = {(uint64_t)2 * G::PITCH, (uint64_t)N * N};
-      const uint64_t strides[1] = {row};
-      const uint32_t box[2] = {bw, bh};
-      e = encode_tensor_map(&map, 2, a.spec, dims, strides, box, (int)sizeof(T));
-    }
-    if (e) {  // surfaces as the launch error of an empty grid
-      rcol_kernel<N, KIND, T><<<0, 1, 0, st>>>(a.spec, a.tw, a.k2tab, a.ctrl, map);
-      return;
-    }
+  memset(map, 0, sizeof(*map));
+  if constexpr (!RCfg<N, T>::pf_single(KIND)) return cudaSuccess;
+  const uint64_t row = (uint64_t)G::PITCH * sizeof(typename C2<T>::t);
+  const uint32_t bh = (uint32_t)rcol_box_rows<N>(), bw = (uint32_t)(2 * G::CC);
+  if (KIND == 2) {
+    const uint64_t dims[3] = {(uint64_t)2 * G::PITCH, (uint64_t)N, (uint64_t)N};
+    const uint64_t strides[2] = {row, row * N};
+    const uint32_t box[3] = {bw, 1, bh};
+    return encode_tensor_map(map, 3, spec, dims, strides, box, (int)sizeof(T));
   }
-  rcol_kernel<N, KIND, T><<<rcolgrid<N, KIND, T, false>(), RCfg<N, T>::NT,
-                             rcolsmem<N, KIND, T, RCfg<N, T>::pf_single(KIND)>(), st>>>(a.spec, a.tw, a.k2tab, a.ctrl,
-                                                                                       map);
+  const uint64_t dims[2] = {(uint64_t)2 * G::PITCH, (uint64_t)N * N};
+  const uint64_t strides[1] = {row};
+  const uint32_t box[2] = {bw, bh};
+  return encode_tensor_map(map, 2, spec, dims, strides, box, (int)sizeof(T));
+}
+
+template <int N, int KIND, class T> static void launch_col(const PoissonArgs<T>& a, cudaStream_t st) {
+  CUtensorMap map;
+  if (col_map<N, KIND, T>(&map, a.spec)) {  // surfaces as the launch error of an empty grid
+    rcol_kernel<N, KIND, T><<<0, 1, 0, st>>>(a.spec, a.tw, a.k2tab, a.ctrl, map);
+    return;
+  }
+  rcol_kernel<N, KIND, T><<<rcolgrid<N, KIND, T, false>(), RCfg<N, T>::NT, rcolsmem<N, KIND, T>(), st>>>(
+      a.spec, a.tw, a.k2tab, a.ctrl, map);
 }
 template <int N, int KIND, class T>
 static void launch_col_b(const SlotArgs<T>* slots, int nslots, int which, cudaStream_t st) {
@@ -911,6 +923,22 @@ cudaError_t launch_poisson_stage(int n, const PoissonArgs<T>& a, int stage, cuda
       return cudaErrorInvalidValue;
   }
 }
+template <class T> cudaError_t encode_column_maps(SlotMaps* m, const void* spec, int n) {
+  cudaError_t e;
+  switch (n) {
+#define CM_CASE(NN)                                                        \
+  case NN:                                                                 \
+    if ((e = col_map<NN, 0, T>(&m->col_y, spec))) return e;                \
+    return col_map<NN, 2, T>(&m->col_z, spec);
+    MHIT_FOR_SIZES(CM_CASE)
+#undef CM_CASE
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+template cudaError_t encode_column_maps<double>(SlotMaps*, const void*, int);
+template cudaError_t encode_column_maps<float>(SlotMaps*, const void*, int);
+
 template cudaError_t launch_poisson_stage<double>(int, const PoissonArgs<double>&, int, cudaStream_t);
 template cudaError_t launch_poisson_stage<float>(int, const PoissonArgs<float>&, int, cudaStream_t);
 

@@ -192,11 +192,6 @@ template <class T> struct PhaseGeo {
 };
 static_assert(PhaseGeo<double>::EX == 36 && PhaseGeo<float>::EX == 40, "staged phi box widths");
 
-// Tensor maps of the staged fields (2D views: x by y*z rows), passed to the
-// kernel as a __grid_constant__ parameter.
-struct PlaneMaps {
-  CUtensorMap u, v, w, phi;
-};
 
 // 1/(sqrt(s) + tiny) for s > 0, the normalisation of A5.  With r = rsqrt(s),
 // 1/(sqrt(s) + tiny) = r/(1 + tiny*r) = r - tiny*r^2 + r*O((tiny*r)^2); the
@@ -210,9 +205,11 @@ __device__ __forceinline__ T inv_norm_plus(T s, T tiny) {
   return (T)1 / (sqrt(s) + tiny);
 }
 
+// phimap: a __grid_constant__ parameter (single simulation), or a map in the
+// ensemble's slot table (gmaps: acquired through the tensor-map proxy first).
 template <class T, bool TMA>
 __device__ __forceinline__ void phase_body(const StencilArgs<T>& a, int KZ, int bx, int by, int bz,
-                                           const CUtensorMap* __restrict__ phimap) {
+                                           const CUtensorMap* __restrict__ phimap, bool gmaps) {
   if (a.ctrl->status) return;
   constexpr int TY = PTY, NT = PNT;
   // The psi ring covers the tile and its 2-cell ring (LX x EY cells); phi and
@@ -283,6 +280,7 @@ __device__ __forceinline__ void phase_body(const StencilArgs<T>& a, int KZ, int 
 #pragma unroll
       for (int q = 0; q < 5; ++q) mbar_init(s_bar + q, 1);
       mbar_init_fence();
+      if (gmaps) tensormap_acquire(phimap);
     }
     __syncthreads();
   }
@@ -451,7 +449,7 @@ __device__ __forceinline__ void phase_body(const StencilArgs<T>& a, int KZ, int 
 // momentum tile height: 8 or 16 rows (a tuning choice per grid size)
 template <class T, bool PF, int MTYv, bool TMA>
 __device__ __forceinline__ void momentum_body(const StencilArgs<T>& a, int KZ, int bx, int by, int bz,
-                                              const PlaneMaps* __restrict__ maps) {
+                                              const PlaneMaps* __restrict__ maps, bool gmaps) {
   if (a.ctrl->status) return;
   // MPT output rows per thread (rows ty + 8h): 256 threads for either tile
   constexpr int TY = MTYv, MPT = MTYv / 8, NT = TX * 8;
@@ -514,6 +512,12 @@ __device__ __forceinline__ void momentum_body(const StencilArgs<T>& a, int KZ, i
 #pragma unroll
       for (int q2 = 0; q2 < NS; ++q2) mbar_init(s_bar + q2, 1);
       mbar_init_fence();
+      if (gmaps) {  // maps in the ensemble's slot table
+        tensormap_acquire(&maps->u);
+        tensormap_acquire(&maps->v);
+        tensormap_acquire(&maps->w);
+        if (PF) tensormap_acquire(&maps->phi);
+      }
     }
     __syncthreads();
   }
@@ -999,12 +1003,12 @@ __device__ __forceinline__ void finalize_body(const double* __restrict__ partial
 template <class T>
 __global__ void __launch_bounds__(PNT, phase_min_blocks<T>())
     phase_kernel(StencilArgs<T> a, int KZ, const __grid_constant__ CUtensorMap phimap) {
-  phase_body<T, true>(a, KZ, blockIdx.x, blockIdx.y, blockIdx.z, &phimap);
+  phase_body<T, true>(a, KZ, blockIdx.x, blockIdx.y, blockIdx.z, &phimap, false);
 }
 template <class T, bool PF, int MTYv>
 __global__ void __launch_bounds__(TX * 8, momentum_min_blocks<T>(PF, MTYv))
     momentum_kernel(StencilArgs<T> a, int KZ, const __grid_constant__ PlaneMaps maps) {
-  momentum_body<T, PF, MTYv, true>(a, KZ, blockIdx.x, blockIdx.y, blockIdx.z, &maps);
+  momentum_body<T, PF, MTYv, true>(a, KZ, blockIdx.x, blockIdx.y, blockIdx.z, &maps, false);
 }
 template <class T, int PKZ>
 __global__ void __launch_bounds__(NT, 4) project_kernel(StencilArgs<T> a) {
@@ -1030,7 +1034,7 @@ __global__ void __launch_bounds__(PNT, phase_min_blocks<T>()) phase_kernel_b(con
   const int par = (int)(a.ctrl->nstep & 1);
   a.phi_in = slots[sl].phi[par];
   a.phi_out = slots[sl].phi[par ^ 1];
-  phase_body<T, false>(a, KZ, blockIdx.x, blockIdx.y, blockIdx.z - sl * zch, nullptr);
+  phase_body<T, true>(a, KZ, blockIdx.x, blockIdx.y, blockIdx.z - sl * zch, &slots[sl].maps.phase_phi[par], true);
 }
 template <class T, bool PF, int MTYv>
 __global__ void __launch_bounds__(TX * 8, momentum_min_blocks<T>(PF, MTYv)) momentum_kernel_b(const SlotArgs<T>* __restrict__ slots, int KZ,
@@ -1038,8 +1042,10 @@ __global__ void __launch_bounds__(TX * 8, momentum_min_blocks<T>(PF, MTYv)) mome
   const int sl = blockIdx.z / zch;
   if (!slots[sl].active) return;
   StencilArgs<T> a = slots[sl].st;
-  if (PF) a.phi_in = slots[sl].phi[(int)((a.ctrl->nstep + 1) & 1)];  // the updated phi
-  momentum_body<T, PF, MTYv, false>(a, KZ, blockIdx.x, blockIdx.y, blockIdx.z - sl * zch, nullptr);
+  const int par = (int)((a.ctrl->nstep + 1) & 1);
+  if (PF) a.phi_in = slots[sl].phi[par];  // the updated phi
+  momentum_body<T, PF, MTYv, true>(a, KZ, blockIdx.x, blockIdx.y, blockIdx.z - sl * zch,
+                                   &slots[sl].maps.mom[MTYv == 16 ? 1 : 0][par], true);
 }
 template <class T, int PKZ>
 __global__ void __launch_bounds__(NT, 4) project_kernel_b(const SlotArgs<T>* __restrict__ slots, int zch) {
@@ -1165,6 +1171,24 @@ template <class T, int TYv> static cudaError_t momentum_maps(PlaneMaps* pm, cons
   if (pf && (e = plane_map(&pm->phi, a.phi_in, n, G::EX, G::EY))) return e;
   return cudaSuccess;
 }
+
+// A served-ensemble slot's tensor maps: the momentum boxes for both tile
+// heights and both phi parities, the phase kernel's phi box per parity, and
+// the column passes' spectrum views.
+template <class T> cudaError_t encode_slot_maps(SlotArgs<T>* s, int n, bool pf) {
+  cudaError_t e;
+  StencilArgs<T> a = s->st;
+  a.c.n = n;
+  for (int par = 0; par < 2; ++par) {
+    a.phi_in = pf ? s->phi[par] : nullptr;
+    if ((e = momentum_maps<T, 8>(&s->maps.mom[0][par], a, pf))) return e;
+    if ((e = momentum_maps<T, 16>(&s->maps.mom[1][par], a, pf))) return e;
+    if (pf && (e = plane_map(&s->maps.phase_phi[par], s->phi[par], n, PhaseGeo<T>::EX, PTY + 4))) return e;
+  }
+  return encode_column_maps<T>(&s->maps, s->po.spec, n);
+}
+template cudaError_t encode_slot_maps<double>(SlotArgs<double>*, int, bool);
+template cudaError_t encode_slot_maps<float>(SlotArgs<float>*, int, bool);
 
 int stencil_size_ok(int n) {
   return n >= 32 && n % TX == 0 && n % TY == 0 && n % PTY == 0 && n % project_kz(n) == 0 && n % pick_kz(n) == 0;
