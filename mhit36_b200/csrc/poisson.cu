@@ -166,6 +166,9 @@ template <int N, class T> struct RCfg {
   // through L1 measured slower for the y passes and no faster for the z
   // solve).
   static constexpr bool pf_single(int kind) { return sizeof(T) == 8 || kind == 2; }
+  // the ensemble's batched passes: FP64 only (the FP32 batched z solve spills
+  // with the prefetch, and its served stream ran 28% slower)
+  static constexpr bool pf_batched(int) { return sizeof(T) == 8; }
   static constexpr bool stw(int) { return true; }
   // (12 elements per thread: y passes 128 in FP64 and 80 in FP32, z solves
   // 168 and 128.)
@@ -342,8 +345,8 @@ __global__ void __launch_bounds__(RCfg<N, T>::NT, RCfg<N, T>::minb(KIND)) rcol_k
   for (int q = 0; q < nslots && !tw; ++q)
     if (slots[q].active) tw = (which ? slots[q].pr : slots[q].po).tw;
   if (!tw) return;
-  constexpr bool PFS = RCfg<N, T>::pf_single(KIND);
-  rcol_run<N, KIND, T, PFS, PFS>(per * nslots, tw, [&](int it) {
+  constexpr bool PFB = RCfg<N, T>::pf_batched(KIND);
+  rcol_run<N, KIND, T, PFB, PFB>(per * nslots, tw, [&](int it) {
     const int sl = it / per;
     const PoissonArgs<T>& a = which ? slots[sl].pr : slots[sl].po;
     ColSlab s;
@@ -766,7 +769,7 @@ template <int N, int KIND, class T, bool BATCHED> static int rcolgrid() {
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (BATCHED)
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, rcol_kernel_b<N, KIND, T>, RCfg<N, T>::NT,
-                                                    rcolsmem<N, KIND, T>());
+                                                    rcolsmem<N, KIND, T, RCfg<N, T>::pf_batched(KIND)>());
     else
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, rcol_kernel<N, KIND, T>, RCfg<N, T>::NT,
                                                     rcolsmem<N, KIND, T, RCfg<N, T>::pf_single(KIND)>());
@@ -811,7 +814,8 @@ template <int N, int KIND, class T> static void launch_col(const PoissonArgs<T>&
 }
 template <int N, int KIND, class T>
 static void launch_col_b(const SlotArgs<T>* slots, int nslots, int which, cudaStream_t st) {
-  rcol_kernel_b<N, KIND, T><<<rcolgrid<N, KIND, T, true>(), RCfg<N, T>::NT, rcolsmem<N, KIND, T>(), st>>>(
+  rcol_kernel_b<N, KIND, T><<<rcolgrid<N, KIND, T, true>(), RCfg<N, T>::NT,
+                               rcolsmem<N, KIND, T, RCfg<N, T>::pf_batched(KIND)>(), st>>>(
       slots, nslots, which);
 }
 
@@ -826,7 +830,9 @@ template <int N, class T> static cudaError_t set_attrs() {
   if ((e = cudaFuncSetAttribute(xfwd_kernel_b<N, 2, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, xs))) return e;
   if ((e = cudaFuncSetAttribute(xinv_kernel_b<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, xs))) return e;
   {
-    const int r0 = (int)rcolsmem<N, 0, T>(), r1 = (int)rcolsmem<N, 1, T>(), r2 = (int)rcolsmem<N, 2, T>();
+    const int r0 = (int)rcolsmem<N, 0, T, RCfg<N, T>::pf_batched(0)>(),
+              r1 = (int)rcolsmem<N, 1, T, RCfg<N, T>::pf_batched(1)>(),
+              r2 = (int)rcolsmem<N, 2, T, RCfg<N, T>::pf_batched(2)>();
     const cudaFuncAttribute A = cudaFuncAttributeMaxDynamicSharedMemorySize;
     const int q0 = (int)rcolsmem<N, 0, T, RCfg<N, T>::pf_single(0)>(),
               q1 = (int)rcolsmem<N, 1, T, RCfg<N, T>::pf_single(1)>(),
