@@ -9,7 +9,7 @@ summed over replicas).  `e2e` is the same metric through the public API with
 host buffers: the upload of the state from pinned host memory, K steps each
 returning its diagnostics to the host, and the download of the state.
 
-On one GPU the line also carries the north star's two other forms:
+On one GPU the line also carries the library's two other forms:
 `fp32_refine` (the FP32 + FP64-residual refinement form on the same workload:
 its step time, speed-up over the FP64 form and per-kernel roofline, and its
 errors against the FP64 form of the same discrete problem after the same
@@ -482,7 +482,7 @@ def main():
 
     mem_bytes = s.memory_bytes()
     s.close()
-    # the other two forms of the north star, on one GPU only: the FP32
+    # the library's two other forms, on one GPU only: the FP32
     # refinement form on the same workload, and a bounded served stream
     fp32 = serving = None
     if world == 1 and args.precision == "fp64" and not args.no_fp32:
