@@ -192,8 +192,7 @@ static size_t rcolsmem() {  // exchange buffer, twiddle table, prefetch buffer
 }
 
 template <int N, int KIND, class T, bool PF, bool TMA, class Getter>
-__device__ __forceinline__ void rcol_run(int total, const typename C2<T>::t* __restrict__ gtw, Getter get,
-                                         int = 0) {
+__device__ __forceinline__ void rcol_run(int total, const typename C2<T>::t* __restrict__ gtw, Getter get) {
   typedef typename C2<T>::t C;
   constexpr int CC = RCfg<N, T>::CC, E = RCfg<N, T>::E, TPC = N / E;
   extern __shared__ __align__(128) unsigned char smem_raw[];
